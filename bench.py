@@ -1,0 +1,332 @@
+"""Benchmark of the contraction engine on one B200 (or N replicas under torchrun).
+
+Workload: the permuted 4-index Float64 contraction
+    C[a,b,c,d] = 1.3 * sum_{e,f} A[a,e,b,f] * B[f,c,e,d] + 0.7 * C[a,b,c,d]
+with a=b=c=d=64, e=f=48 (M = N = 4096, K = 2304), A and B iid uniform[-1,1]
+from a seeded generator, C seeded N(0,1), column-major (Julia layout).  One
+step = one ``execute`` of a reused plan (pack + tensor-core GEMM + epilogue).
+Inputs (A 75 MB, B 75 MB, C 268 MB) are larger than the 126 MB L2, so no
+explicit flush runs between steps.
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the CPU arm: the
+oracle's restatement of the reference's five-loop nest (QuasiStrided.jl is
+Julia and cannot run here) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZES = dict(a=64, b=64, c=64, d=64, e=48, f=48)
+LABELS = dict(indA=(1, 5, 2, 6), indB=(6, 3, 5, 4), indC=(1, 2, 3, 4))
+ALPHA, BETA = 1.3, 0.7
+M = N = 64 * 64
+K = 48 * 48
+FLOPS = 2.0 * M * N * K
+WORKLOAD = "permuted4_f64_M4096_N4096_K2304"
+
+
+def load_engine():
+    pkg = os.path.join(ROOT, "quasistrided.jl_b200")
+    if "quasistrided_b200" in sys.modules:
+        return sys.modules["quasistrided_b200"]
+    spec = importlib.util.spec_from_file_location("quasistrided_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["quasistrided_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def shapes():
+    s = SIZES
+    return ((s["a"], s["e"], s["b"], s["f"]), (s["f"], s["c"], s["e"], s["d"]),
+            (s["a"], s["b"], s["c"], s["d"]))
+
+
+def host_inputs(seed=20261203, wide=False):
+    """Seeded column-major inputs (flat float64 arrays)."""
+    rng = np.random.default_rng(seed)
+    sa, sb, sc = shapes()
+    A = rng.uniform(-1.0, 1.0, int(np.prod(sa)))
+    B = rng.uniform(-1.0, 1.0, int(np.prod(sb)))
+    C = rng.standard_normal(int(np.prod(sc)))
+    if wide:
+        ua = rng.integers(-20, 21, sa[0]).astype(np.float64)
+        ud = rng.integers(-20, 21, sb[3]).astype(np.float64)
+        A = (A.reshape(sa, order="F") * np.exp2(ua)[:, None, None, None]).ravel(order="F")
+        B = (B.reshape(sb, order="F") * np.exp2(ud)[None, None, None, :]).ravel(order="F")
+    return A, B, C
+
+
+def colmajor_strides(shape):
+    st, acc = [], 1
+    for s in shape:
+        st.append(acc)
+        acc *= s
+    return tuple(st)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.idx = device_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_sample(orc, A, B, C, rows, threads):
+    """Time the oracle's nest restatement on `rows` rows of M (c1 layout)."""
+    sa, sb, sc = shapes()
+    Av = orc.HostView(A, sa, colmajor_strides(sa))
+    Bv = orc.HostView(B, sb, colmajor_strides(sb))
+    Cv = orc.HostView(C.copy(), sc, colmajor_strides(sc))
+    t0 = time.perf_counter()
+    orc.nest_f64(Cv, ALPHA, Av, LABELS["indA"], Bv, LABELS["indB"], BETA, LABELS["indC"],
+                 m_range=(0, rows), threads=threads)
+    dt = time.perf_counter() - t0
+    return 2.0 * rows * N * K / dt / 1e12, dt
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the oracle's nest restatement on all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    threads = orc.max_threads()
+    A, B, C = host_inputs()
+    rows = args.cpu_rows
+    for _ in range(args.warmup):
+        cpu_sample(orc, A, B, C, max(64, rows // 8), threads)
+    vals, times = [], []
+    for _ in range(args.steps):
+        v, dt = cpu_sample(orc, A, B, C, rows, threads)
+        vals.append(v)
+        times.append(dt)
+    value = statistics.median(vals)
+    sample = f"{rows} of {M} rows of M (all N, all K) per step, oracle nest restatement, {threads} threads"
+    print(json.dumps({
+        "impl": "reference", "metric": "contraction TFLOP/s (Float64, rel.err<=1e-13 vs FP64)",
+        "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1] A/B, N(0,1) C)",
+        "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "alpha": ALPHA, "beta": BETA,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--method", default="auto", choices=["auto", "native", "ozaki"])
+    ap.add_argument("--cpu-rows", type=int, default=512)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    qs = load_engine()
+    dev = torch.device("cuda", local)
+
+    A_h, B_h, C_h = host_inputs(seed=20261203 + rank)
+    sa, sb, sc = shapes()
+    Ad = torch.from_numpy(A_h).to(dev)
+    Bd = torch.from_numpy(B_h).to(dev)
+    C0d = torch.from_numpy(C_h).to(dev)
+    Cd = C0d.clone()
+    Av = qs.StridedView(Ad, sa, colmajor_strides(sa), 0)
+    Bv = qs.StridedView(Bd, sb, colmajor_strides(sb), 0)
+    Cv = qs.StridedView(Cd, sc, colmajor_strides(sc), 0)
+    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method)
+
+    # Accuracy of the measured path: one execution from the seeded C against
+    # the FP64 oracle on a sample of C elements (first 2 rows of each 64-block
+    # of M... i.e. the leading elements of C in memory order).
+    from oracle import oracle as orc
+    qs.execute(plan, ALPHA, BETA)
+    torch.cuda.synchronize()
+    got = Cd.cpu().numpy()
+    nsamp = 8192
+    Cref = orc.HostView(C_h.copy(), sc, colmajor_strides(sc))
+    orc.brute(Cref, ALPHA, orc.HostView(A_h, sa, colmajor_strides(sa)), LABELS["indA"],
+              orc.HostView(B_h, sb, colmajor_strides(sb)), LABELS["indB"], BETA, LABELS["indC"],
+              c_range=(0, nsamp))
+    ref = Cref.parent[:nsamp]
+    rel_err = float(np.linalg.norm(got[:nsamp] - ref) / np.linalg.norm(ref))
+
+    stream = torch.cuda.current_stream()
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        qs.execute(plan, ALPHA, BETA)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = qs._abi.lib().qs_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            qs.execute(plan, ALPHA, BETA)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = qs._abi.lib().qs_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * FLOPS / (ms * 1e-3) / 1e12
+
+    # Dominant kernel's own duration: the plan's GEMM stage, timed alone.
+    kern = qs.kernel_profile(plan, ALPHA, BETA, reps=max(3, args.steps // 2)) if hasattr(qs, "kernel_profile") else None
+    peaks, peak_kind = measured_peaks()
+    if kern is not None:
+        roof = kern
+    else:
+        roof = {"bound": "tensor", "achieved": value, "peak": None, "unit": "TFLOP/s", "frac": None,
+                "traffic": None}
+
+    # End to end through the public API with host buffers.
+    A_p = torch.from_numpy(A_h).pin_memory()
+    B_p = torch.from_numpy(B_h).pin_memory()
+    C_p = torch.from_numpy(C_h).pin_memory()
+    C_out = torch.empty_like(C_p).pin_memory()
+    h2d = (A_p.numel() + B_p.numel() + C_p.numel()) * 8
+    d2h = C_out.numel() * 8
+    for _ in range(1):
+        Ad.copy_(A_p, non_blocking=True); Bd.copy_(B_p, non_blocking=True); Cd.copy_(C_p, non_blocking=True)
+        qs.execute(plan, ALPHA, BETA)
+        C_out.copy_(Cd, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        Ad.copy_(A_p, non_blocking=True); Bd.copy_(B_p, non_blocking=True); Cd.copy_(C_p, non_blocking=True)
+        qs.execute(plan, ALPHA, BETA)
+        C_out.copy_(Cd, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * FLOPS / (e2e_ms * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, dt = cpu_sample(orc, A_h, B_h, C_h, args.cpu_rows, orc.max_threads())
+        cpu = {"value": v, "unit": "TFLOP/s", "cores": orc.max_threads(), "kind": "port",
+               "sample": f"{args.cpu_rows} of {M} rows of M through the oracle's nest restatement ({dt:.1f} s)"}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": "contraction TFLOP/s (Float64, rel.err<=1e-13 vs FP64)",
+            "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1] A/B, N(0,1) C)",
+            "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "alpha": ALPHA, "beta": BETA,
+                       "method": plan.method, "ozaki_slices": plan.ozaki_slices,
+                       "l2": "inputs larger than L2 (419 MB), no flush", "parallelism": f"replicas{world}"},
+            "rel_err": rel_err, "rel_err_sample": nsamp,
+            "roofline": roof, "peaks_source": peak_kind,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }), flush=True)
+    plan.release()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,207 @@
+/*
+ * qsgpu.h — C ABI of the B200 contraction engine (libqsgpu.so).
+ *
+ * Computes C[indC] = alpha * sum_K op(A)[indA] * op(B)[indB] + beta * C[indC]
+ * over strided ("block-scatter") operands that live in device memory, with
+ * the semantics of QuasiStrided.jl's engine:
+ *
+ *   plan_contract  src/planning/plan.jl:115-133   -> qs_plan_contract
+ *   execute!       src/execution/execute.jl:191   -> qs_execute
+ *   contract!      src/execution/execute.jl:264   -> qs_contract
+ *   release!       src/execution/workspace.jl:118 -> qs_plan_destroy
+ *   QuasiStridedBackend(; accumulator)            -> qs_plan_options.accumulator
+ *     src/integrations/tensoroperations.jl:299-307
+ *   TO.tensorcontract! label mapping              -> qs_contraction_labels
+ *     src/integrations/tensoroperations.jl:315-322
+ *
+ * Conventions
+ *  - Every operand is a qs_view: a parent allocation (`data`, `length`
+ *    elements) plus a StridedView-style (size, strides, offset, op) window
+ *    into it; strides are in elements and may be zero or negative
+ *    (StridedViews.jl's StridedView fields).
+ *  - Labels are one int64 per axis, as in the reference (`indA`, `indB`,
+ *    `indC`): a label in A and B but not C is contracted (K); a label in C
+ *    and exactly one of A/B is free (M or N).  Any other pattern is QS_EINVAL.
+ *  - Scalars (alpha, beta) are passed as two doubles {re, im}; for a real
+ *    compute type a nonzero imaginary part is QS_EINVAL (Julia's
+ *    `convert(T, alpha)` throws InexactError).
+ *  - Every validation happens before anything is written: plan-time errors
+ *    come from qs_plan_contract, out-of-bounds operands from qs_execute before
+ *    any launch (src/execution/execute.jl:182-189,
+ *    test/execution/test_execute.jl:334-347).
+ *  - No C++ exception crosses this boundary.  The message of the last error
+ *    on the calling thread is available from qs_last_error.
+ *  - A plan borrows the operands' device memory and owns its device
+ *    workspace (offset tables, packed panels).  One stream per execute; a plan
+ *    must not be executed concurrently with itself (src/planning/plan.jl:12).
+ */
+#ifndef QSGPU_H
+#define QSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The Julia/Python hosts map them to the reference's exception
+ * types: EINVAL -> ArgumentError, EDIM -> DimensionMismatch,
+ * EBOUNDS -> BoundsError. */
+enum {
+  QS_OK = 0,
+  QS_EINVAL = 1,   /* ArgumentError: labels, eltypes, conjugated C, aliasing */
+  QS_EDIM = 2,     /* DimensionMismatch: a label's axis lengths differ */
+  QS_EBOUNDS = 3,  /* BoundsError: a view reaches outside its parent */
+  QS_ENOMEM = 4,   /* device allocation failed (plan time only) */
+  QS_ETIMEOUT = 5, /* a device-side bounded wait gave up (status flag) */
+  QS_ECUDA = 6,    /* a CUDA runtime call failed */
+  QS_ENOTSUP = 7   /* requested method/kernel not available for this plan */
+};
+
+/* Element types: QuasiStrided's SUPPORTED_ELTYPES (src/planning/plan.jl:264). */
+enum { QS_F32 = 0, QS_F64 = 1, QS_C32 = 2, QS_C64 = 3 };
+
+/* StridedView.op (src/planning/plan.jl:176-186). */
+enum { QS_OP_IDENTITY = 0, QS_OP_CONJ = 1, QS_OP_TRANSPOSE = 2, QS_OP_ADJOINT = 3 };
+
+/* accumulator keyword: nothing / Float32 / Float64 (src/planning/plan.jl:278-285). */
+enum { QS_ACC_NONE = 0, QS_ACC_F32 = 1, QS_ACC_F64 = 2 };
+
+/* GEMM method for the nest path.  AUTO follows the autotuner's choice. */
+enum {
+  QS_METHOD_AUTO = 0,
+  QS_METHOD_NATIVE = 1,   /* plain FP64 DMMA / FP32 FFMA gather kernel */
+  QS_METHOD_OZAKI_I8 = 2, /* FP64 as INT8 slices on tcgen05 kind::i8 */
+  QS_METHOD_BF16X3 = 3    /* FP32 as split-BF16 x3 on tcgen05 kind::f16 */
+};
+
+/* Path modes (src/planning/plan.jl:60-64 PathModes). */
+enum { QS_MODE_AUTO = 0, QS_MODE_NEVER = 1, QS_MODE_ALWAYS = 2 };
+
+/* Execution paths (src/execution/paths.jl). */
+enum {
+  QS_PATH_EMPTY = 0,
+  QS_PATH_SCALE = 1,
+  QS_PATH_DOT = 2,
+  QS_PATH_OUTER = 3,
+  QS_PATH_NEST = 4
+};
+
+/* Complex formulations on the real tensor-core paths. */
+enum { QS_CPLX_NONE = 0, QS_CPLX_PLANAR = 1, QS_CPLX_1M = 2 };
+
+/* Plan flags. */
+enum {
+  QS_PLAN_HOST_ONLY = 1 /* plan on the host only: no device workspace; the
+                           plan can be inspected but not executed */
+};
+
+typedef struct qs_view {
+  void *data;             /* device pointer to element 0 of the parent */
+  int64_t length;         /* parent length in elements */
+  int64_t offset;         /* element offset of the view's first element */
+  const int64_t *size;    /* [ndim] */
+  const int64_t *strides; /* [ndim], in elements */
+  int32_t ndim;
+  int32_t eltype; /* QS_F32 .. QS_C64 */
+  int32_t op;     /* QS_OP_* */
+  int32_t reserved;
+} qs_view;
+
+typedef struct qs_plan_options {
+  int32_t conjA;       /* conjugate A's elements (XOR with A's op) */
+  int32_t conjB;       /* conjugate B's elements (XOR with B's op) */
+  int32_t accumulator; /* QS_ACC_* */
+  int32_t method;      /* QS_METHOD_* */
+  int64_t m_block;     /* blocking hints (src/planning/blocking.jl:9-20): */
+  int64_t k_block;     /* 0 = default; values < 0 are QS_EINVAL.  On the */
+  int64_t n_block;     /* device they only bound the K segment length.   */
+  int32_t dot_mode;    /* QS_MODE_* */
+  int32_t outer_mode;  /* QS_MODE_* */
+  int32_t unpacked_b_mode; /* QS_MODE_* (read-B-in-place skinny path) */
+  int32_t ozaki_slices;    /* 0 = chosen from K for 1e-13; else 2..10 */
+  int32_t complex_mode;    /* QS_CPLX_*; 0 = default for the method */
+  int32_t flags;           /* QS_PLAN_* */
+} qs_plan_options;
+
+typedef struct qs_plan_info {
+  int32_t path;         /* QS_PATH_* */
+  int32_t method;       /* QS_METHOD_* actually used by the nest path */
+  int32_t compute_type; /* QS_F32 .. QS_C64 */
+  int32_t swapped;      /* 1 when B takes the M role */
+  int32_t conjA;        /* effective conjugation of the M-side operand */
+  int32_t conjB;        /* effective conjugation of the N-side operand */
+  int32_t ozaki_slices;
+  int32_t complex_mode;
+  int64_t m_length, n_length, k_length;
+  int32_t m_rank, n_rank, k_rank;
+  int32_t bounds_ok; /* 0 when qs_execute would return QS_EBOUNDS */
+  int64_t m_labels[16], n_labels[16], k_labels[16]; /* group label order */
+  int64_t workspace_bytes;
+} qs_plan_info;
+
+typedef struct qs_plan qs_plan;
+
+/* plan_contract (src/planning/plan.jl:115-133).  indA/indB/indC hold
+ * A->ndim, B->ndim, C->ndim labels.  opts may be NULL (all defaults). */
+int qs_plan_contract(qs_plan **plan, const qs_view *C, const qs_view *A,
+                     const int64_t *indA, const qs_view *B,
+                     const int64_t *indB, const int64_t *indC,
+                     const qs_plan_options *opts);
+
+/* execute! (src/execution/execute.jl:191-200): alpha/beta are {re, im}.
+ * stream is a cudaStream_t (NULL = legacy default stream).  Asynchronous:
+ * returns once the work is enqueued. */
+int qs_execute(qs_plan *plan, const double *alpha, const double *beta,
+               void *stream);
+
+/* contract! (src/execution/execute.jl:264-275): plan, execute, release in one
+ * call.  The plan's workspace is freed stream-ordered after the work. */
+int qs_contract(const qs_view *C, const double *alpha, const qs_view *A,
+                const int64_t *indA, const qs_view *B, const int64_t *indB,
+                const double *beta, const int64_t *indC,
+                const qs_plan_options *opts, void *stream);
+
+/* release! (src/execution/workspace.jl:118-123) plus freeing the plan. */
+int qs_plan_destroy(qs_plan *plan);
+
+/* Inspection of a plan (path, groups, method) for hosts and tests. */
+int qs_plan_get_info(const qs_plan *plan, qs_plan_info *info);
+
+/* Re-point a plan at new operand storage of identical layout (same parent
+ * lengths, offsets): src/planning/plan.jl:48-56 rebuilds a plan with new
+ * storages the same way.  Used by the serving loop to reuse plans. */
+int qs_plan_rebind(qs_plan *plan, void *A_data, void *B_data, void *C_data);
+
+/* TO.tensorcontract! label mapping (src/integrations/tensoroperations.jl:315-322):
+ * pA = (pA_out[NoA], pA_in[Nk]), pB = (pB_in[Nk], pB_out[NoB]),
+ * pAB = (pAB_1 ++ pAB_2)[NoA+NoB], all 1-based as in Julia.  Writes
+ * indA[NoA+Nk], indB[Nk+NoB], indC[NoA+NoB]. */
+int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB,
+                          const int64_t *pA_lin, const int64_t *pB_lin,
+                          const int64_t *pAB_lin, int64_t *indA,
+                          int64_t *indB, int64_t *indC);
+
+/* Grouped execution of many independent plans as one persistent launch over
+ * a device problem table (block-sparse contractions).  All plans must be of
+ * the same compute type; alpha/beta are per plan ({re, im} pairs, 2*n
+ * doubles each). */
+int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha,
+                       const double *beta, void *stream);
+
+/* Number of device kernels this library has launched in this process
+ * (instrumentation: benchmarks difference it around a timed region). */
+int64_t qs_launch_count(void);
+
+/* Message of the last error on this thread; returns its full length. */
+size_t qs_last_error(char *buf, size_t n);
+
+/* Library version string. */
+const char *qs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSGPU_H */

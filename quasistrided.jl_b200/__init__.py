@@ -1,0 +1,395 @@
+"""Host-side mirror of QuasiStrided.jl's engine API over the B200 C-ABI library.
+
+Names, argument meaning and error behaviour follow the reference:
+
+====================  ==========================================================
+this module           QuasiStrided.jl
+====================  ==========================================================
+``StridedView``       ``StridedViews.StridedView`` (parent, size, strides, offset, op)
+``plan_contract``     ``plan_contract`` (src/planning/plan.jl:115-133)
+``execute``           ``execute!`` (src/execution/execute.jl:191-200)
+``contract``          ``contract!`` (src/execution/execute.jl:264-275)
+``ContractPlan``      ``ContractPlan`` (src/planning/plan.jl:16-45)
+``release``           ``release!`` (src/execution/workspace.jl:118-123)
+``PathModes``         ``PathModes`` (src/planning/plan.jl:60-64)
+``QuasiStridedBackend``  ``QuasiStridedBackend`` (src/integrations/tensoroperations.jl:299-307)
+``tensorcontract``    ``TO.tensorcontract!`` method (tensoroperations.jl:350-363)
+``contraction_labels``  ``contraction_labels`` (tensoroperations.jl:315-322)
+====================  ==========================================================
+
+Operands are ``StridedView`` s over torch tensors in device memory.  All
+compute happens in libqsgpu.so's sm_100a kernels; there is no CPU fallback:
+a missing library or a non-CUDA operand raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import torch
+
+from . import _abi
+from ._abi import (ArgumentError, BoundsError, DimensionMismatch, EngineError,  # noqa: F401
+                   QS_C32, QS_C64, QS_F32, QS_F64)
+
+__all__ = [
+    "StridedView", "plan_contract", "execute", "contract", "ContractPlan", "PathModes",
+    "QuasiStridedBackend", "tensorcontract", "contraction_labels", "release",
+    "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "colmajor",
+    "execute_grouped",
+]
+
+_DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
+                torch.complex64: QS_C32, torch.complex128: QS_C64}
+_OPS = ("identity", "conj", "transpose", "adjoint")
+
+
+def _eltype(dtype: torch.dtype) -> int:
+    try:
+        return _DTYPE_TO_QS[dtype]
+    except KeyError:
+        raise ArgumentError(
+            f"plan_contract: eltype {dtype}; each must be one of Float32, Float64, "
+            "ComplexF32, ComplexF64") from None
+
+
+class StridedView:
+    """A strided window (size, strides, offset, op) into a flat parent tensor.
+
+    ``StridedView(t)`` wraps a torch tensor with its own size/strides/offset;
+    ``StridedView(parent, size, strides, offset, op)`` builds one explicitly
+    (StridedViews.jl's five-argument constructor).  Strides are in elements
+    and may be zero or negative; nothing checks the window against the
+    parent here — ``execute`` does, before any write.
+    """
+
+    def __init__(self, parent: torch.Tensor, size: Optional[Sequence[int]] = None,
+                 strides: Optional[Sequence[int]] = None, offset: Optional[int] = None,
+                 op: str = "identity"):
+        if not isinstance(parent, torch.Tensor):
+            raise ArgumentError("StridedView parent must be a torch.Tensor")
+        if op not in _OPS:
+            raise ArgumentError(
+                f"unsupported StridedView.op {op}: QuasiStrided folds a view's `op` into the "
+                "packing transform and recognizes only identity/conj/transpose/adjoint")
+        if size is None:
+            size, strides = tuple(parent.shape), tuple(parent.stride())
+            offset = parent.storage_offset() if offset is None else offset
+            n = parent.untyped_storage().nbytes() // parent.element_size()
+            flat = torch.as_strided(parent, (n,), (1,), 0)
+        else:
+            if strides is None:
+                raise ArgumentError("StridedView: strides are required with size")
+            flat = parent.reshape(-1) if parent.dim() != 1 else parent
+            offset = 0 if offset is None else offset
+        self.parent = flat
+        self.size = tuple(int(s) for s in size)
+        self.strides = tuple(int(s) for s in strides)
+        if len(self.size) != len(self.strides):
+            raise ArgumentError("StridedView: size and strides differ in length")
+        self.offset = int(offset)
+        self.op = op
+
+    @property
+    def dtype(self):
+        return self.parent.dtype
+
+    @property
+    def ndim(self):
+        return len(self.size)
+
+    def permutedims(self, perm: Sequence[int]) -> "StridedView":
+        """permutedims(view, perm), 0-based perm."""
+        return StridedView(self.parent, [self.size[p] for p in perm],
+                           [self.strides[p] for p in perm], self.offset, self.op)
+
+    def with_op(self, op: str) -> "StridedView":
+        return StridedView(self.parent, self.size, self.strides, self.offset, op)
+
+    def to_tensor(self) -> torch.Tensor:
+        """Materialise the window (applying a conjugating op), for tests."""
+        t = torch.as_strided(self.parent, self.size, self.strides, self.offset) if self.size else \
+            self.parent[self.offset:self.offset + 1].reshape(())
+        if self.op in ("conj", "adjoint") and t.is_complex():
+            t = t.conj()
+        return t.resolve_conj()
+
+    def _c(self, keep: list) -> _abi.qs_view:
+        size = (ctypes.c_int64 * max(1, len(self.size)))(*self.size)
+        strides = (ctypes.c_int64 * max(1, len(self.strides)))(*self.strides)
+        keep.extend([size, strides])
+        v = _abi.qs_view()
+        v.data = self.parent.data_ptr()
+        v.length = self.parent.numel()
+        v.offset = self.offset
+        v.size = size
+        v.strides = strides
+        v.ndim = len(self.size)
+        v.eltype = _eltype(self.parent.dtype)
+        v.op = _abi.QS_OP[self.op]
+        return v
+
+
+def colmajor(shape: Sequence[int], dtype=torch.float64, device="cuda", fill=None,
+             generator=None) -> StridedView:
+    """A dense column-major (Julia layout) array as a StridedView."""
+    n = 1
+    for s in shape:
+        n *= int(s)
+    if fill is None:
+        parent = torch.zeros(max(n, 1), dtype=dtype, device=device)
+    else:
+        parent = torch.full((max(n, 1),), fill, dtype=dtype, device=device)
+    strides, acc = [], 1
+    for s in shape:
+        strides.append(acc)
+        acc *= int(s)
+    return StridedView(parent, tuple(shape), tuple(strides), 0)
+
+
+@dataclass(frozen=True)
+class PathModes:
+    """Overrides for the dot / outer-product / read-B-in-place paths
+    (``:auto``/``:never``/``:always`` in the reference)."""
+    dot: str = "auto"
+    outer: str = "auto"
+    unpacked_b: str = "auto"
+
+
+def _acc_code(accumulator) -> int:
+    if accumulator in (None, "nothing"):
+        return 0
+    if accumulator in ("Float32", torch.float32):
+        return 1
+    if accumulator in ("Float64", torch.float64):
+        return 2
+    raise ArgumentError(
+        f"QuasiStridedBackend: accumulator must be nothing, Float32 or Float64, got {accumulator}")
+
+
+def _scalar(x) -> ctypes.Array:
+    if isinstance(x, torch.Tensor):
+        x = x.item()
+    z = complex(x)
+    return (ctypes.c_double * 2)(z.real, z.imag)
+
+
+class ContractPlan:
+    """Reusable plan: M/N/K groups, path, method and the device workspace.
+
+    The plan borrows the operands' storage (it keeps the Python objects
+    alive) and owns its workspace until ``release``.  One execution at a time.
+    """
+
+    def __init__(self, handle, C, A, B, host_only):
+        self._h = handle
+        self.C, self.A, self.B = C, A, B
+        self.host_only = host_only
+        info = _abi.qs_plan_info()
+        _abi.check(_abi.lib().qs_plan_get_info(handle, ctypes.byref(info)))
+        self.path = _abi.QS_PATH_NAME[info.path]
+        self.method = _abi.QS_METHOD_NAME[info.method]
+        self.compute_type = _abi.ELTYPE_NAME[info.compute_type]
+        self.swapped = bool(info.swapped)
+        self.conjA, self.conjB = bool(info.conjA), bool(info.conjB)
+        self.ozaki_slices = info.ozaki_slices
+        self.complex_mode = {0: None, 1: "planar", 2: "1m"}[info.complex_mode]
+        self.m_length, self.n_length, self.k_length = info.m_length, info.n_length, info.k_length
+        self.m_labels = tuple(info.m_labels[:info.m_rank])
+        self.n_labels = tuple(info.n_labels[:info.n_rank])
+        self.k_labels = tuple(info.k_labels[:info.k_rank])
+        self.bounds_ok = bool(info.bounds_ok)
+        self.workspace_bytes = info.workspace_bytes
+
+    @property
+    def Cstorage(self) -> torch.Tensor:
+        return self.C.parent
+
+    def release(self) -> None:
+        if self._h:
+            _abi.lib().qs_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def __repr__(self):
+        return (f"ContractPlan({self.compute_type}, {self.path}, method={self.method}, "
+                f"M={self.m_length}, N={self.n_length}, K={self.k_length}, swapped={self.swapped})")
+
+
+def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=None,
+             k_block=None, n_block=None, path_modes: Optional[PathModes] = None,
+             ozaki_slices=0, complex_mode=None, host_only=False) -> _abi.qs_plan_options:
+    o = _abi.qs_plan_options()
+    o.conjA, o.conjB = int(bool(conjA)), int(bool(conjB))
+    o.accumulator = _acc_code(accumulator)
+    if method not in _abi.QS_METHOD:
+        raise ArgumentError(f"unknown method {method!r}")
+    o.method = _abi.QS_METHOD[method]
+    for name, val in (("m_block", m_block), ("k_block", k_block), ("n_block", n_block)):
+        if val is not None and int(val) < 1:
+            raise ArgumentError(f"{name} must be >= 1, got {val}")
+        setattr(o, name, 0 if val is None else int(val))
+    pm = path_modes or PathModes()
+    o.dot_mode = _abi.QS_MODE[pm.dot]
+    o.outer_mode = _abi.QS_MODE[pm.outer]
+    o.unpacked_b_mode = _abi.QS_MODE[pm.unpacked_b]
+    o.ozaki_slices = int(ozaki_slices)
+    o.complex_mode = _abi.QS_CPLX[complex_mode]
+    o.flags = _abi.QS_PLAN_HOST_ONLY if host_only else 0
+    return o
+
+
+def _labels(ind: Sequence[int], n: int, name: str, keep: list):
+    ind = tuple(int(x) for x in ind)
+    if len(ind) != n:
+        raise ArgumentError(f"{name} has {len(ind)} labels for a rank-{n} operand")
+    arr = (ctypes.c_int64 * max(1, n))(*ind)
+    keep.append(arr)
+    return arr
+
+
+def _check_device(host_only: bool, *views: StridedView) -> None:
+    if host_only:
+        return
+    for v in views:
+        if not v.parent.is_cuda:
+            raise ArgumentError("operands must live in CUDA device memory (no CPU fallback)")
+
+
+def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, indC, *,
+                  kernel=None, conjA=False, conjB=False, m_block=None, k_block=None,
+                  n_block=None, allocator=None, accumulator=None,
+                  path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
+                  complex_mode=None, host_only=False) -> ContractPlan:
+    """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
+
+    Throws ArgumentError / DimensionMismatch on invalid input, before any
+    device work.  ``kernel`` names a method ("native", "ozaki", "bf16x3");
+    ``allocator`` is accepted for signature parity (the plan allocates its
+    workspace in device memory).  ``host_only`` plans without touching the
+    device (inspection only).
+    """
+    if kernel is not None:
+        method = kernel
+    _check_device(host_only, C, A, B)
+    keep: list = []
+    cC, cA, cB = C._c(keep), A._c(keep), B._c(keep)
+    iA = _labels(indA, A.ndim, "indA", keep)
+    iB = _labels(indB, B.ndim, "indB", keep)
+    iC = _labels(indC, C.ndim, "indC", keep)
+    o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
+                 ozaki_slices, complex_mode, host_only)
+    h = ctypes.c_void_p()
+    _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
+                                           ctypes.byref(cB), iB, iC, ctypes.byref(o)))
+    return ContractPlan(h, C, A, B, host_only)
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def execute(plan: ContractPlan, alpha, beta, stream=None) -> torch.Tensor:
+    """``execute!``: C = alpha*A*B + beta*C for the plan; returns C's storage.
+
+    beta applies exactly once and beta == 0 never reads C; alpha == 0 or an
+    empty K never reads A or B; an out-of-bounds operand raises BoundsError
+    before any write.  Enqueued on ``stream`` (default: torch's current).
+    """
+    if plan._h is None:
+        raise ArgumentError("plan has been released")
+    a, b = _scalar(alpha), _scalar(beta)
+    s = None if plan.host_only else _stream_ptr(stream)
+    _abi.check(_abi.lib().qs_execute(plan._h, a, b, s))
+    return plan.Cstorage
+
+
+def release(plan: ContractPlan, allocator=None) -> None:
+    """``release!``: free the plan's device workspace."""
+    plan.release()
+
+
+def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, beta, indC, *,
+             accumulator=None, conjA=False, conjB=False, method="auto", stream=None) -> StridedView:
+    """``contract!``: plan, execute, release; returns C."""
+    _check_device(False, C, A, B)
+    keep: list = []
+    cC, cA, cB = C._c(keep), A._c(keep), B._c(keep)
+    iA = _labels(indA, A.ndim, "indA", keep)
+    iB = _labels(indB, B.ndim, "indB", keep)
+    iC = _labels(indC, C.ndim, "indC", keep)
+    o = _options(conjA, conjB, accumulator, method)
+    _abi.check(_abi.lib().qs_contract(ctypes.byref(cC), _scalar(alpha), ctypes.byref(cA), iA,
+                                      ctypes.byref(cB), iB, _scalar(beta), iC, ctypes.byref(o),
+                                      _stream_ptr(stream)))
+    return C
+
+
+def execute_grouped(plans: Sequence[ContractPlan], alphas, betas, stream=None) -> None:
+    """Execute many independent plans as grouped launches (block-sparse steps)."""
+    n = len(plans)
+    arr = (ctypes.c_void_p * max(1, n))(*[p._h for p in plans])
+    al = (ctypes.c_double * (2 * max(1, n)))()
+    be = (ctypes.c_double * (2 * max(1, n)))()
+    for i in range(n):
+        za, zb = complex(alphas[i]), complex(betas[i])
+        al[2 * i], al[2 * i + 1] = za.real, za.imag
+        be[2 * i], be[2 * i + 1] = zb.real, zb.imag
+    _abi.check(_abi.lib().qs_execute_grouped(n, arr, al, be, _stream_ptr(stream)))
+
+
+# ------------------------------------------------------- TensorOperations ---
+
+def contraction_labels(pA, pB, pAB):
+    """TO's (pA, pB, pAB) index tuples (1-based) -> (indA, indB, indC)."""
+    NoA, Nk = len(pA[0]), len(pA[1])
+    NoB = len(pB[1])
+    if len(pB[0]) != Nk:
+        raise ArgumentError("pA and pB disagree on the number of contracted indices")
+    lin = lambda p: tuple(p[0]) + tuple(p[1])  # noqa: E731
+    a, b, c = lin(pA), lin(pB), lin(pAB)
+    mk = lambda xs: (ctypes.c_int64 * max(1, len(xs)))(*xs)  # noqa: E731
+    outA = (ctypes.c_int64 * max(1, NoA + Nk))()
+    outB = (ctypes.c_int64 * max(1, Nk + NoB))()
+    outC = (ctypes.c_int64 * max(1, NoA + NoB))()
+    _abi.check(_abi.lib().qs_contraction_labels(NoA, Nk, NoB, mk(a), mk(b), mk(c), outA, outB, outC))
+    return tuple(outA[:NoA + Nk]), tuple(outB[:Nk + NoB]), tuple(outC[:NoA + NoB])
+
+
+class QuasiStridedBackend:
+    """TensorOperations-style backend running contractions on this engine.
+
+    ``accumulator`` is ``None``, ``"Float32"`` or ``"Float64"`` and is
+    validated at construction, as ``QuasiStridedBackend{A}()`` does.
+    """
+
+    def __init__(self, accumulator=None):
+        _acc_code(accumulator)
+        self.accumulator = accumulator
+
+    def __repr__(self):
+        return f"QuasiStridedBackend(accumulator={self.accumulator})"
+
+
+def tensorcontract(C, A, pA, conjA, B, pB, conjB, pAB, alpha, beta,
+                   backend: QuasiStridedBackend, allocator=None):
+    """``TO.tensorcontract!(C, A, pA, conjA, B, pB, conjB, pAB, α, β, backend)``."""
+    Cv = C if isinstance(C, StridedView) else StridedView(C)
+    Av = A if isinstance(A, StridedView) else StridedView(A)
+    Bv = B if isinstance(B, StridedView) else StridedView(B)
+    if len(pA[0]) + len(pA[1]) != Av.ndim or len(pB[0]) + len(pB[1]) != Bv.ndim or \
+            len(pAB[0]) + len(pAB[1]) != Cv.ndim:
+        raise ArgumentError("invalid permutation of length")
+    indA, indB, indC = contraction_labels(pA, pB, pAB)
+    # dimcheck_tensorcontract: matching extents are checked by the planner.
+    contract(Cv, alpha, Av, indA, Bv, indB, beta, indC, accumulator=backend.accumulator,
+             conjA=conjA, conjB=conjB)
+    return C

@@ -1,0 +1,341 @@
+// The C ABI (include/qsgpu.h): plan creation, execution and destruction.
+//
+//   qs_plan_contract <- plan_contract / planned (src/planning/plan.jl:115-262)
+//   qs_execute       <- execute! (src/execution/execute.jl:191-210)
+//   qs_contract      <- contract! (src/execution/execute.jl:264-275)
+//   qs_plan_destroy  <- release! (src/execution/workspace.jl:118-123)
+//
+// All validation happens on the host before anything is written; kernels
+// are launched asynchronously on the caller's stream.  No exception crosses
+// the boundary.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <sstream>
+#include <vector>
+
+#include "kernels.h"
+#include "qs_internal.h"
+#include "tc.h"
+
+using namespace qs;
+
+#include <atomic>
+
+namespace qs {
+static std::atomic<int64_t> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace qs
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  std::ostringstream s;
+  s << "CUDA error in " << what << ": " << cudaGetErrorString(e);
+  return fail(QS_ECUDA, s.str());
+}
+
+void free_workspace(qs_plan *p) {
+  for (void *q : p->ws.owned) cudaFree(q);
+  p->ws.owned.clear();
+  p->ws = Workspace{};
+}
+
+int ws_alloc(qs_plan *p, void **out, size_t bytes) {
+  *out = nullptr;
+  if (bytes == 0) return QS_OK;
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    std::ostringstream s;
+    s << "device allocation of " << bytes << " bytes failed: " << cudaGetErrorString(e);
+    return fail(QS_ENOMEM, s.str());
+  }
+  p->ws.owned.push_back(*out);
+  p->ws.bytes += bytes;
+  return QS_OK;
+}
+
+int upload_offsets(qs_plan *p, const Group &g, int64_t **dst) {
+  int64_t Q = g.length();
+  size_t n = (size_t)(Q > 0 ? Q : 1);
+  std::vector<int64_t> h(2 * n, 0);
+  if (Q > 0) {
+    g.fill_offsets(0, 0, Q, h.data());
+    g.fill_offsets(1, 0, Q, h.data() + n);
+  }
+  void *d;
+  int rc = ws_alloc(p, &d, 2 * n * sizeof(int64_t));
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpy(d, h.data(), 2 * n * sizeof(int64_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (offset tables)");
+  dst[0] = (int64_t *)d;
+  dst[1] = (int64_t *)d + n;
+  return QS_OK;
+}
+
+Operands make_operands(const qs_plan *p) {
+  Operands op;
+  op.A = p->Adata;
+  op.B = p->Bdata;
+  op.C = p->Cdata;
+  op.Abase = p->Abase;
+  op.Bbase = p->Bbase;
+  op.Cbase = p->Cbase;
+  op.TA = p->TA;
+  op.TB = p->TB;
+  op.TC = p->TC;
+  op.conjA = p->conjA;
+  op.conjB = p->conjB;
+  op.offMA = p->ws.offM[0];
+  op.offMC = p->ws.offM[1];
+  op.offNB = p->ws.offN[0];
+  op.offNC = p->ws.offN[1];
+  op.offKA = p->ws.offK[0];
+  op.offKB = p->ws.offK[1];
+  op.M = p->M;
+  op.N = p->N;
+  op.K = p->K;
+  return op;
+}
+
+// Method for the nest path: the requested one if valid, else the
+// autotuner's choice (tensor-core paths once the problem fills a tile).
+int choose_method(qs_plan *p) {
+  int want = p->opts.method;
+  bool dbl = is_double(p->T);
+  if (want == QS_METHOD_OZAKI_I8 && !dbl)
+    return fail(QS_ENOTSUP, "ArgumentError: the Ozaki INT8 method needs a Float64/ComplexF64 compute type");
+  if (want == QS_METHOD_BF16X3 && dbl)
+    return fail(QS_ENOTSUP, "ArgumentError: the split-BF16x3 method needs a Float32/ComplexF32 compute type");
+  if (want < QS_METHOD_AUTO || want > QS_METHOD_BF16X3)
+    return fail(QS_EINVAL, "ArgumentError: unknown method");
+  if (want == QS_METHOD_AUTO) want = tc_auto_method(p);
+  p->method = want;
+  return QS_OK;
+}
+
+int scalar_case(int T, const double *v) {
+  // Zero/One/general after conversion to the compute type.
+  double re = v[0], im = is_complex(T) ? v[1] : 0.0;
+  if (!is_double(T)) {
+    re = (double)(float)re;
+    im = (double)(float)im;
+  }
+  if (re == 0.0 && im == 0.0) return 0;
+  if (re == 1.0 && im == 0.0) return 1;
+  return 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t qs_last_error(char *buf, size_t n);  // defined below
+
+int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const int64_t *indA,
+                     const qs_view *B, const int64_t *indB, const int64_t *indC,
+                     const qs_plan_options *opts) {
+  if (!out) return fail(QS_EINVAL, "ArgumentError: plan output pointer is NULL");
+  *out = nullptr;
+  qs_plan *p = new (std::nothrow) qs_plan();
+  if (!p) return fail(QS_ENOMEM, "host allocation failed");
+  int rc = plan_host(p, C, A, indA, B, indB, indC, opts);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  if (p->path == QS_PATH_NEST) {
+    rc = choose_method(p);
+    if (rc) {
+      delete p;
+      return rc;
+    }
+  } else {
+    p->method = QS_METHOD_NATIVE;
+  }
+  if (!p->host_only) {
+    cudaError_t e = cudaGetDevice(&p->device);
+    if (e != cudaSuccess) {
+      delete p;
+      return cuda_fail(e, "cudaGetDevice");
+    }
+    if (p->path != QS_PATH_EMPTY) {
+      if ((rc = upload_offsets(p, p->mg, p->ws.offM)) || (rc = upload_offsets(p, p->ng, p->ws.offN)) ||
+          (rc = upload_offsets(p, p->kg, p->ws.offK))) {
+        free_workspace(p);
+        delete p;
+        return rc;
+      }
+    }
+    if (p->path == QS_PATH_NEST && p->method != QS_METHOD_NATIVE) {
+      rc = tc_prepare(p);
+      if (rc) {
+        free_workspace(p);
+        delete p;
+        return rc;
+      }
+    }
+  } else if (p->path == QS_PATH_NEST && p->method != QS_METHOD_NATIVE) {
+    tc_geometry(p);
+  }
+  set_error(QS_OK, "");
+  *out = p;
+  return QS_OK;
+}
+
+int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream) {
+  if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
+  if (!alpha || !beta) return fail(QS_EINVAL, "ArgumentError: alpha/beta is NULL");
+  if (p->host_only)
+    return fail(QS_EINVAL, "ArgumentError: a host-only plan has no device workspace to execute");
+  if (!is_complex(p->T) && (alpha[1] != 0.0 || beta[1] != 0.0))
+    return fail(QS_EINVAL, "InexactError: a complex alpha/beta does not convert to the real compute type");
+  if (!std::isfinite(alpha[0]) && std::isnan(alpha[0])) {
+    // NaN alpha is a legal value: it propagates like the reference.
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int acase = scalar_case(p->T, alpha);
+  int bcase = scalar_case(p->T, beta);
+  if (p->path == QS_PATH_EMPTY) return QS_OK;
+  bool scale_only = (acase == 0) || p->path == QS_PATH_SCALE;
+  int rc = check_bounds(p, !scale_only);
+  if (rc) return rc;
+  cudaSetDevice(p->device);
+  Operands op = make_operands(p);
+  cudaError_t e = cudaSuccess;
+  if (scale_only) {
+    if (bcase == 1) return QS_OK;  // C *= 1 is a no-op
+    e = launch_scale(p->T, op, beta, bcase, p->c_mfast, st);
+    if (e != cudaSuccess) return cuda_fail(e, "scale kernel launch");
+    count_launches(1);
+    return QS_OK;
+  }
+  switch (p->path) {
+    case QS_PATH_DOT: e = launch_dot(p->T, op, alpha, beta, bcase, st); break;
+    case QS_PATH_OUTER: e = launch_outer(p->T, op, alpha, beta, bcase, p->c_mfast, st); break;
+    default:
+      if (p->method == QS_METHOD_NATIVE) {
+        e = launch_direct(p->T, op, alpha, beta, bcase, p->a_mfast, p->b_nfast, st);
+      } else {
+        return tc_execute(p, alpha, beta, bcase, st);
+      }
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  count_launches(1);
+  return QS_OK;
+}
+
+int qs_plan_destroy(qs_plan *p) {
+  if (!p) return QS_OK;
+  if (!p->host_only) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaSetDevice(p->device);
+    free_workspace(p);
+    cudaSetDevice(dev);
+  }
+  delete p;
+  return QS_OK;
+}
+
+int qs_contract(const qs_view *C, const double *alpha, const qs_view *A, const int64_t *indA,
+                const qs_view *B, const int64_t *indB, const double *beta, const int64_t *indC,
+                const qs_plan_options *opts, void *stream) {
+  qs_plan_options o{};
+  if (opts) o = *opts;
+  o.flags &= ~QS_PLAN_HOST_ONLY;
+  qs_plan *p = nullptr;
+  int rc = qs_plan_contract(&p, C, A, indA, B, indB, indC, &o);
+  if (rc) return rc;
+  rc = qs_execute(p, alpha, beta, stream);
+  // The workspace is released once the enqueued work is done.
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  qs_plan_destroy(p);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+  return QS_OK;
+}
+
+int qs_plan_get_info(const qs_plan *p, qs_plan_info *info) {
+  if (!p || !info) return fail(QS_EINVAL, "ArgumentError: NULL argument");
+  std::memset(info, 0, sizeof(*info));
+  info->path = p->path;
+  info->method = p->method;
+  info->compute_type = p->T;
+  info->swapped = p->swapped;
+  info->conjA = p->conjA;
+  info->conjB = p->conjB;
+  info->ozaki_slices = p->ozaki_slices;
+  info->complex_mode = p->complex_mode;
+  info->m_length = p->M;
+  info->n_length = p->N;
+  info->k_length = p->K;
+  info->m_rank = p->mg.D;
+  info->n_rank = p->ng.D;
+  info->k_rank = p->kg.D;
+  info->bounds_ok = p->bounds_ok_c && p->bounds_ok_ab;
+  for (int d = 0; d < p->mg.D; ++d) info->m_labels[d] = p->mg.label[d];
+  for (int d = 0; d < p->ng.D; ++d) info->n_labels[d] = p->ng.label[d];
+  for (int d = 0; d < p->kg.D; ++d) info->k_labels[d] = p->kg.label[d];
+  info->workspace_bytes = (int64_t)p->ws.bytes;
+  return QS_OK;
+}
+
+int qs_plan_rebind(qs_plan *p, void *A_data, void *B_data, void *C_data) {
+  if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
+  void *a = p->swapped ? B_data : A_data;
+  void *b = p->swapped ? A_data : B_data;
+  if (a) p->Adata = a;
+  if (b) p->Bdata = b;
+  if (C_data) p->Cdata = C_data;
+  return QS_OK;
+}
+
+int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB, const int64_t *pA_lin,
+                          const int64_t *pB_lin, const int64_t *pAB_lin, int64_t *indA,
+                          int64_t *indB, int64_t *indC) {
+  // TO's pA/pB/pAB -> one label per axis (src/integrations/tensoroperations.jl:315-322):
+  // 1:NoA for A's open axes (pA[1] order), NoA+1:NoA+NoB for B's open axes,
+  // -1:-1:-Nk for the contracted pairs; indC = linearize(pAB).
+  if (NoA < 0 || Nk < 0 || NoB < 0) return fail(QS_EINVAL, "ArgumentError: negative counts");
+  int nA = NoA + Nk, nB = Nk + NoB;
+  std::vector<int64_t> qA(nA), qB(nB);
+  for (int i = 0; i < nA; ++i) {
+    int64_t ax = pA_lin[i];
+    if (ax < 1 || ax > nA) return fail(QS_EINVAL, "ArgumentError: invalid pA");
+    qA[ax - 1] = i + 1;  // invperm
+  }
+  for (int i = 0; i < nB; ++i) {
+    int64_t ax = pB_lin[i];
+    if (ax < 1 || ax > nB) return fail(QS_EINVAL, "ArgumentError: invalid pB");
+    qB[ax - 1] = i + 1;
+  }
+  for (int i = 0; i < nA; ++i) {
+    int64_t s = qA[i];
+    indA[i] = s <= NoA ? s : -(s - NoA);
+  }
+  for (int i = 0; i < nB; ++i) {
+    int64_t s = qB[i];
+    indB[i] = s <= Nk ? -s : NoA + (s - Nk);
+  }
+  for (int i = 0; i < NoA + NoB; ++i) indC[i] = pAB_lin[i];
+  return QS_OK;
+}
+
+int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha, const double *beta,
+                       void *stream) {
+  if (n < 0 || (n > 0 && (!plans || !alpha || !beta)))
+    return fail(QS_EINVAL, "ArgumentError: invalid grouped arguments");
+  return tc_execute_grouped(n, plans, alpha, beta, (cudaStream_t)stream);
+}
+
+size_t qs_last_error(char *buf, size_t n);
+
+const char *qs_version(void) { return "qsgpu 0.1.0 (sm_100a)"; }
+
+int64_t qs_launch_count(void) { return qs::g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

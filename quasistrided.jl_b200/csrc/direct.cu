@@ -1,0 +1,383 @@
+// Gather kernels that read the operands in place through the plan's offset
+// tables: the plain ("native") GEMM, C *= beta, the dot-product and the
+// outer-product paths.
+//
+//   native GEMM   <- nest!/micro_tiles!/ScalarKernel (src/execution/nest.jl:7-191,
+//                    src/microkernels/steps.jl:27-36): acc = muladd(a, b, acc)
+//                    ascending in the plan's K order; complex in the planar
+//                    kernel's fused order (steps.jl:121-167)
+//   scale         <- scale_all_of_C! (src/execution/execute.jl:214-245)
+//   dot           <- execute_path!(DotPath) (src/execution/dot.jl:13-76)
+//   outer         <- execute_path!(OuterPath) (src/execution/outer.jl:10-69)
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace qs {
+
+// ------------------------------------------------------------- scale ----
+
+template <class T>
+__global__ void scale_kernel(Operands op, Scalars<T> s, int mfast) {
+  int64_t total = op.M * op.N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (mfast) {
+      i = e % op.M;
+      j = e / op.M;
+    } else {
+      j = e % op.N;
+      i = e / op.N;
+    }
+    int64_t idx = op.Cbase + op.offMC[i] + op.offNC[j];
+    T v = s.beta_case == 0 ? tzero<T>() : cmul(load_c<T>(op.C, idx, op.TC), s.beta);
+    store_c<T>(op.C, idx, op.TC, v);
+  }
+}
+
+// -------------------------------------------------------- native GEMM ----
+// Register-tiled gather GEMM: a CTA computes a BM x BN tile of C; each of
+// its 256 threads owns TM x TN outputs.  A/B tiles are gathered through the
+// offset tables (coalesced along whichever axis is unit-stride), converted
+// to the compute type with conjugation on load, and double-buffered in
+// shared memory.  The K loop runs over all of K, so beta is applied once.
+
+template <class T, int BM, int BN, int BK>
+struct DirectCfg {
+  static constexpr int kThreads = 256;
+  static constexpr int TM = BM / 16;
+  static constexpr int TN = BN / 16;
+  static constexpr int A_PER_THREAD = BM * BK / kThreads;
+  static constexpr int B_PER_THREAD = BN * BK / kThreads;
+};
+
+template <class T, int BM, int BN, int BK>
+__global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T> s, int a_mfast,
+                                                          int b_nfast) {
+  using Cfg = DirectCfg<T, BM, BN, BK>;
+  constexpr int TM = Cfg::TM, TN = Cfg::TN;
+  __shared__ T As[2][BK][BM];
+  __shared__ T Bs[2][BK][BN];
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = tzero<T>();
+
+  T ra[Cfg::A_PER_THREAD], rb[Cfg::B_PER_THREAD];
+  auto a_coord = [&](int r, int &mm, int &kk) {
+    int e = tid + r * Cfg::kThreads;
+    if (a_mfast) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+  };
+  auto b_coord = [&](int r, int &nn, int &kk) {
+    int e = tid + r * Cfg::kThreads;
+    if (b_nfast) { nn = e % BN; kk = e / BN; } else { kk = e % BK; nn = e / BK; }
+  };
+  auto gather = [&](int64_t k0) {
+#pragma unroll
+    for (int r = 0; r < Cfg::A_PER_THREAD; ++r) {
+      int mm, kk;
+      a_coord(r, mm, kk);
+      int64_t m = m0 + mm, k = k0 + kk;
+      ra[r] = (m < op.M && k < op.K)
+                  ? Loader<T>::load(op.A, op.Abase + op.offMA[m] + op.offKA[k], op.TA, op.conjA)
+                  : tzero<T>();
+    }
+#pragma unroll
+    for (int r = 0; r < Cfg::B_PER_THREAD; ++r) {
+      int nn, kk;
+      b_coord(r, nn, kk);
+      int64_t n = n0 + nn, k = k0 + kk;
+      rb[r] = (n < op.N && k < op.K)
+                  ? Loader<T>::load(op.B, op.Bbase + op.offNB[n] + op.offKB[k], op.TB, op.conjB)
+                  : tzero<T>();
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < Cfg::A_PER_THREAD; ++r) {
+      int mm, kk;
+      a_coord(r, mm, kk);
+      As[buf][kk][mm] = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < Cfg::B_PER_THREAD; ++r) {
+      int nn, kk;
+      b_coord(r, nn, kk);
+      Bs[buf][kk][nn] = rb[r];
+    }
+  };
+
+  const int64_t nkb = (op.K + BK - 1) / BK;
+  gather(0);
+  stash(0);
+  __syncthreads();
+  for (int64_t kb = 0; kb < nkb; ++kb) {
+    const int cur = kb & 1;
+    if (kb + 1 < nkb) gather((kb + 1) * BK);
+    const int64_t krem = op.K - kb * BK;
+    const int kmax = krem < BK ? (int)krem : BK;
+    for (int kk = 0; kk < kmax; ++kk) {
+      T a[TM], b[TN];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) a[i] = As[cur][kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) b[j] = Bs[cur][kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
+    }
+    if (kb + 1 < nkb) stash(cur ^ 1);
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    int64_t m = m0 + ty + 16 * i;
+    if (m >= op.M) continue;
+    int64_t cm = op.Cbase + op.offMC[m];
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      int64_t n = n0 + tx + 16 * j;
+      if (n >= op.N) continue;
+      int64_t idx = cm + op.offNC[n];
+      T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
+      store_c<T>(op.C, idx, op.TC, axpby(s, acc[i][j], old));
+    }
+  }
+}
+
+// ---------------------------------------------------------------- dot ----
+// out[q] = alpha * sum_k X[q,k] * v[k] + beta * C[q] for M == 1 or N == 1.
+// kmode = 1: one warp per output, lanes stride K (K unit-stride in X);
+// kmode = 0: one thread per output (Q unit-stride in X).
+
+struct DotArgs {
+  const void *X;  // matrix operand
+  const void *V;  // vector operand
+  int64_t Xbase, Vbase;
+  int TX, TV;
+  int conjX, conjV;
+  const int64_t *offQX, *offKX, *offKV, *offQC;
+  int x_is_a;  // X plays A (product a*b = X*v) or B (v*X)
+  int64_t Q, K;
+  void *C;
+  int64_t Cbase;
+  int TC;
+};
+
+template <class T>
+__device__ __forceinline__ T dot_term(const DotArgs &d, int64_t q, int64_t k) {
+  T x = Loader<T>::load(d.X, d.Xbase + d.offQX[q] + d.offKX[k], d.TX, d.conjX);
+  T v = Loader<T>::load(d.V, d.Vbase + d.offKV[k], d.TV, d.conjV);
+  return d.x_is_a ? cmul(x, v) : cmul(v, x);
+}
+
+template <class T>
+__device__ __forceinline__ T shfl_down_t(T v, int o) {
+  if constexpr (is_cplx<T>::value) {
+    v.re = __shfl_down_sync(0xffffffffu, v.re, o);
+    v.im = __shfl_down_sync(0xffffffffu, v.im, o);
+    return v;
+  } else {
+    return __shfl_down_sync(0xffffffffu, v, o);
+  }
+}
+template <class T>
+__device__ __forceinline__ T tadd(T a, T b) {
+  if constexpr (is_cplx<T>::value) {
+    a.re += b.re;
+    a.im += b.im;
+    return a;
+  } else {
+    return a + b;
+  }
+}
+
+template <class T>
+__global__ void dot_kernel(DotArgs d, Scalars<T> s, int kmode) {
+  if (kmode) {
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32;
+    int lane = threadIdx.x & 31;
+    int64_t nwarps = (int64_t)gridDim.x * blockDim.x / 32;
+    for (int64_t q = warp; q < d.Q; q += nwarps) {
+      T acc = tzero<T>();
+      for (int64_t k = lane; k < d.K; k += 32) {
+        T x = Loader<T>::load(d.X, d.Xbase + d.offQX[q] + d.offKX[k], d.TX, d.conjX);
+        T v = Loader<T>::load(d.V, d.Vbase + d.offKV[k], d.TV, d.conjV);
+        acc = d.x_is_a ? cfma(x, v, acc) : cfma(v, x, acc);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc = tadd(acc, shfl_down_t(acc, o));
+      if (lane == 0) {
+        int64_t idx = d.Cbase + d.offQC[q];
+        T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(d.C, idx, d.TC);
+        store_c<T>(d.C, idx, d.TC, axpby(s, acc, old));
+      }
+    }
+  } else {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < d.Q;
+         q += (int64_t)gridDim.x * blockDim.x) {
+      T acc = tzero<T>();
+      const int64_t xq = d.Xbase + d.offQX[q];
+      for (int64_t k = 0; k < d.K; ++k) {
+        T x = Loader<T>::load(d.X, xq + d.offKX[k], d.TX, d.conjX);
+        T v = Loader<T>::load(d.V, d.Vbase + d.offKV[k], d.TV, d.conjV);
+        acc = d.x_is_a ? cfma(x, v, acc) : cfma(v, x, acc);
+      }
+      int64_t idx = d.Cbase + d.offQC[q];
+      T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(d.C, idx, d.TC);
+      store_c<T>(d.C, idx, d.TC, axpby(s, acc, old));
+    }
+  }
+}
+
+// -------------------------------------------------------------- outer ----
+// K == 1: C[i,j] = alpha * (a_i * b_j) + beta * C[i,j]; r = a*b then the
+// store expression, term for term as the nest (src/execution/outer.jl:1-8).
+
+template <class T>
+__global__ void outer_kernel(Operands op, Scalars<T> s, int mfast) {
+  int64_t total = op.M * op.N;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (mfast) { i = e % op.M; j = e / op.M; } else { j = e % op.N; i = e / op.N; }
+    T a = Loader<T>::load(op.A, op.Abase + op.offMA[i] + op.offKA[0], op.TA, op.conjA);
+    T b = Loader<T>::load(op.B, op.Bbase + op.offNB[j] + op.offKB[0], op.TB, op.conjB);
+    T r = cmul(a, b);
+    int64_t idx = op.Cbase + op.offMC[i] + op.offNC[j];
+    T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
+    store_c<T>(op.C, idx, op.TC, axpby(s, r, old));
+  }
+}
+
+// ------------------------------------------------------------ launchers ---
+
+static int grid_for(int64_t work, int threads) {
+  int64_t g = (work + threads - 1) / threads;
+  int64_t cap = 148 * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+template <class T>
+static Scalars<T> make_scalars(const double *alpha, const double *beta, int beta_case) {
+  Scalars<T> s;
+  if constexpr (is_cplx<T>::value) {
+    using R = typename real_of<T>::type;
+    s.alpha.re = (R)alpha[0];
+    s.alpha.im = (R)alpha[1];
+    s.beta.re = (R)beta[0];
+    s.beta.im = (R)beta[1];
+  } else {
+    s.alpha = (T)alpha[0];
+    s.beta = (T)beta[0];
+  }
+  s.beta_case = beta_case;
+  return s;
+}
+
+template <class T>
+static cudaError_t launch_scale_t(const Operands &op, const double *alpha, const double *beta,
+                                  int beta_case, int mfast, cudaStream_t st) {
+  auto s = make_scalars<T>(alpha, beta, beta_case);
+  scale_kernel<T><<<grid_for(op.M * op.N, 256), 256, 0, st>>>(op, s, mfast);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(int T, const Operands &op, const double *beta, int beta_case, int mfast,
+                         cudaStream_t st) {
+  const double zero[2] = {0, 0};
+  switch (T) {
+    case QS_F32: return launch_scale_t<float>(op, zero, beta, beta_case, mfast, st);
+    case QS_F64: return launch_scale_t<double>(op, zero, beta, beta_case, mfast, st);
+    case QS_C32: return launch_scale_t<cplx<float>>(op, zero, beta, beta_case, mfast, st);
+    default: return launch_scale_t<cplx<double>>(op, zero, beta, beta_case, mfast, st);
+  }
+}
+
+template <class T, int BM, int BN, int BK>
+static cudaError_t launch_direct_t(const Operands &op, const double *alpha, const double *beta,
+                                   int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
+  auto s = make_scalars<T>(alpha, beta, beta_case);
+  dim3 grid((unsigned)((op.M + BM - 1) / BM), (unsigned)((op.N + BN - 1) / BN));
+  direct_gemm_kernel<T, BM, BN, BK><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct(int T, const Operands &op, const double *alpha, const double *beta,
+                          int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
+  switch (T) {
+    case QS_F32: return launch_direct_t<float, 64, 64, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_F64: return launch_direct_t<double, 64, 64, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_C32: return launch_direct_t<cplx<float>, 32, 32, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    default: return launch_direct_t<cplx<double>, 32, 32, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+  }
+}
+
+template <class T>
+static cudaError_t launch_dot_t(const DotArgs &d, const double *alpha, const double *beta,
+                                int beta_case, int kmode, cudaStream_t st) {
+  auto s = make_scalars<T>(alpha, beta, beta_case);
+  int threads = 256;
+  int64_t work = kmode ? d.Q * 32 : d.Q;
+  dot_kernel<T><<<grid_for(work, threads), threads, 0, st>>>(d, s, kmode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dot(int T, const Operands &op, const double *alpha, const double *beta,
+                       int beta_case, cudaStream_t st) {
+  DotArgs d;
+  if (op.N == 1) {  // X = A (Q = M), v = B
+    d.X = op.A; d.V = op.B; d.Xbase = op.Abase; d.Vbase = op.Bbase + 0;
+    d.TX = op.TA; d.TV = op.TB; d.conjX = op.conjA; d.conjV = op.conjB;
+    d.offQX = op.offMA; d.offKX = op.offKA; d.offKV = op.offKB; d.offQC = op.offMC;
+    d.x_is_a = 1; d.Q = op.M;
+    d.Vbase = op.Bbase;  // the single N coordinate has offset 0
+  } else {          // M == 1: X = B (Q = N), v = A
+    d.X = op.B; d.V = op.A; d.Xbase = op.Bbase; d.Vbase = op.Abase;
+    d.TX = op.TB; d.TV = op.TA; d.conjX = op.conjB; d.conjV = op.conjA;
+    d.offQX = op.offNB; d.offKX = op.offKB; d.offKV = op.offKA; d.offQC = op.offNC;
+    d.x_is_a = 0; d.Q = op.N;
+  }
+  d.K = op.K;
+  d.C = op.C;
+  d.Cbase = op.Cbase;
+  d.TC = op.TC;
+  int kmode = 1;  // default: warp per output
+  switch (T) {
+    case QS_F32: return launch_dot_t<float>(d, alpha, beta, beta_case, kmode, st);
+    case QS_F64: return launch_dot_t<double>(d, alpha, beta, beta_case, kmode, st);
+    case QS_C32: return launch_dot_t<cplx<float>>(d, alpha, beta, beta_case, kmode, st);
+    default: return launch_dot_t<cplx<double>>(d, alpha, beta, beta_case, kmode, st);
+  }
+}
+
+template <class T>
+static cudaError_t launch_outer_t(const Operands &op, const double *alpha, const double *beta,
+                                  int beta_case, int mfast, cudaStream_t st) {
+  auto s = make_scalars<T>(alpha, beta, beta_case);
+  outer_kernel<T><<<grid_for(op.M * op.N, 256), 256, 0, st>>>(op, s, mfast);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const double *beta,
+                         int beta_case, int mfast, cudaStream_t st) {
+  switch (T) {
+    case QS_F32: return launch_outer_t<float>(op, alpha, beta, beta_case, mfast, st);
+    case QS_F64: return launch_outer_t<double>(op, alpha, beta, beta_case, mfast, st);
+    case QS_C32: return launch_outer_t<cplx<float>>(op, alpha, beta, beta_case, mfast, st);
+    default: return launch_outer_t<cplx<double>>(op, alpha, beta, beta_case, mfast, st);
+  }
+}
+
+}  // namespace qs

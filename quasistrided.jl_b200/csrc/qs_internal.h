@@ -1,0 +1,125 @@
+// Internal declarations shared by the host planner (planner.cpp), the C ABI
+// (api.cu) and the kernel translation units.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "../../include/qsgpu.h"
+
+namespace qs {
+
+constexpr int kMaxRank = 16;  // labels per M/N/K composite
+
+// A grouped tensor axis: D dims enumerated by one zero-based coordinate,
+// first dim fastest, with two stride maps (src/layout/axis_group.jl:5-23).
+// Map 0/1 are (A, C) for M, (B, C) for N and (A, B) for K.
+struct Group {
+  int D = 0;
+  int64_t len[kMaxRank] = {};
+  int64_t st[2][kMaxRank] = {};
+  int64_t label[kMaxRank] = {};
+  int64_t length() const {
+    int64_t q = 1;
+    for (int d = 0; d < D; ++d) q *= len[d];
+    return q;
+  }
+  // (lo, hi) of map p's offsets over the whole group; (0, -1) when empty.
+  void offset_range(int p, int64_t &lo, int64_t &hi) const;
+  // Step of map p when it is a single ramp (offset(q) = q*step), else
+  // sets ok=false (src/layout/axis_group.jl:149-168).
+  int64_t ramp_step(int p, bool &ok) const;
+  // Mixed-radix offsets of coordinates [first, first+count) of map p
+  // (src/layout/axis_group.jl:87-145).
+  void fill_offsets(int p, int64_t first, int64_t count, int64_t *out) const;
+};
+
+struct Status {
+  int code = QS_OK;
+  std::string msg;
+};
+
+// Thread-local last error used by qs_last_error.
+void set_error(int code, const std::string &msg);
+int fail(int code, const std::string &msg);
+
+inline bool is_complex(int t) { return t == QS_C32 || t == QS_C64; }
+inline bool is_double(int t) { return t == QS_F64 || t == QS_C64; }
+inline int elsize(int t) {
+  switch (t) {
+    case QS_F32: return 4;
+    case QS_F64: return 8;
+    case QS_C32: return 8;
+    case QS_C64: return 16;
+  }
+  return 0;
+}
+const char *eltype_name(int t);
+
+// Device workspace of a plan: offset tables and packed panels.  Owned by the
+// plan, allocated at plan time, freed by qs_plan_destroy.
+struct Workspace {
+  // offset tables, device int64: M maps (A, C), N maps (B, C), K maps (A, B)
+  int64_t *offM[2] = {nullptr, nullptr};
+  int64_t *offN[2] = {nullptr, nullptr};
+  int64_t *offK[2] = {nullptr, nullptr};
+  // tensor-core paths: packed operand panels and per-row/col exponents
+  void *panelA = nullptr;
+  void *panelB = nullptr;
+  int32_t *expA = nullptr;  // per packed row of A (Ozaki), or nullptr
+  int32_t *expB = nullptr;
+  int32_t *status = nullptr;  // device status word (bounded waits)
+  size_t bytes = 0;
+  std::vector<void *> owned;  // every cudaMalloc'd pointer, for freeing
+};
+
+struct TensorCoreGeom {
+  // Padded problem in packed-panel units.
+  int64_t Mp = 0, Np = 0, Kp = 0;  // padded rows of A/B panels and K
+  int64_t mtiles = 0, ntiles = 0, kblocks = 0;
+  int rows_per_elem_a = 1;  // 1m: 2 real rows per complex row of A
+  int kmul = 1;             // 1m: 2 real K per complex K
+  int nslices = 0;          // Ozaki slices (or 2 planes hi/lo for bf16x3)
+  int64_t plane_bytes_a = 0, plane_bytes_b = 0;
+  int kseg = 0;             // K blocks per INT32-exact segment (Ozaki)
+};
+
+}  // namespace qs
+
+struct qs_plan {
+  // Operand roles after the optional swap: "A" feeds M, "B" feeds N.
+  int TA = 0, TB = 0, TC = 0;
+  int T = 0;  // compute type
+  int conjA = 0, conjB = 0;  // effective conjugation (flag XOR op), per role
+  int swapped = 0;
+  void *Adata = nullptr, *Bdata = nullptr, *Cdata = nullptr;
+  int64_t Alen = 0, Blen = 0, Clen = 0;
+  int64_t Abase = 0, Bbase = 0, Cbase = 0;
+  qs::Group mg, ng, kg;
+  int64_t M = 0, N = 0, K = 0;
+  int path = QS_PATH_EMPTY;
+  int method = QS_METHOD_NATIVE;
+  int complex_mode = QS_CPLX_NONE;
+  int ozaki_slices = 0;
+  int bounds_ok_c = 1, bounds_ok_ab = 1;
+  std::string bounds_msg;
+  int host_only = 0;
+  int device = 0;
+  qs_plan_options opts{};
+  // Per-path launch flags chosen at plan time.
+  int a_mfast = 0;  // A's M map is unit-stride (gather along M)
+  int b_nfast = 0;  // B's N map is unit-stride (gather along N)
+  int c_mfast = 0;  // C's M map is unit-stride
+  qs::TensorCoreGeom tc;
+  qs::Workspace ws;
+};
+
+namespace qs {
+// planner.cpp
+int plan_host(qs_plan *p, const qs_view *C, const qs_view *A,
+              const int64_t *indA, const qs_view *B, const int64_t *indB,
+              const int64_t *indC, const qs_plan_options *opts);
+int check_bounds(const qs_plan *p, bool reads_ab);
+}  // namespace qs
