@@ -1,15 +1,728 @@
-// Tensor-core paths: placeholder until the kernels land.
+// Tensor-core paths of the nest (execute_path!(NestPath), src/execution/nest.jl:7-191):
+//
+//  * Float64 as an Ozaki-style split: every row of A and every column of B is
+//    scaled by a power of two (its max-magnitude exponent), cut into s signed
+//    7-bit integer slices, and the slice products are computed exactly on the
+//    integer tensor cores (tcgen05.mma kind::i8, INT32 accumulation in TMEM).
+//    Products of equal weight (p + q = t) share one INT32 accumulator; each
+//    diagonal is added into an FP64 running sum kept in TMEM, and the final
+//    alpha/beta epilogue rescales and rounds once to eltype(C).
+//  * Float32 as split-BF16 x3: hi = bf16(x), lo = bf16(x - hi); the products
+//    hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM (kind::f16).
+//
+// Packing (src/packing/pack.jl:43-99) becomes a device pass that gathers each
+// operand through its offset tables, converts it to the compute type with
+// conjugation on load, and writes K-major panels in the exact byte image of
+// the 128-byte-swizzled shared-memory tiles the MMA reads, so the GEMM moves
+// whole tiles with single bulk copies.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <vector>
+
 #include "kernels.h"
+#include "ptx.cuh"
 #include "tc.h"
 
 namespace qs {
 
-int tc_auto_method(const qs_plan *) { return QS_METHOD_NATIVE; }
-void tc_geometry(qs_plan *) {}
-int tc_prepare(qs_plan *) { return fail(QS_ENOTSUP, "tensor-core path not built"); }
-int tc_execute(qs_plan *, const double *, const double *, int, cudaStream_t) {
-  return fail(QS_ENOTSUP, "tensor-core path not built");
+constexpr int kTileM = 128;     // UMMA M
+constexpr int kKBytes = 128;    // bytes of K per panel tile (one swizzle row)
+constexpr int kNonFinite = INT_MIN;
+
+// ------------------------------------------------------------- packing ---
+
+struct PackArgs {
+  const void *X;
+  int64_t Xbase;
+  int TX, conj;
+  const int64_t *offR, *offK;  // row (M or N) and K offset tables of X
+  int64_t rows, K;             // logical extents
+  int64_t rows_pad;            // padded to the panel tile height
+  int tile_rows;               // 128 or 256
+  int kblocks;                 // K bytes / 128 per padded row
+  int rfast;                   // rows are X's unit-stride axis
+  uint8_t *panel;
+  int64_t plane;  // bytes per slice plane
+  int nslices;
+  int32_t *exp_out;
+  int32_t *flag_list, *flag_count;
+};
+
+__device__ __forceinline__ int64_t panel_tile_base(const PackArgs &a, int64_t row, int64_t kbyte) {
+  int64_t rt = row / a.tile_rows, r = row % a.tile_rows;
+  int64_t kb = kbyte >> 7;
+  return ((rt * a.kblocks + kb) * a.tile_rows) * kKBytes + sw128_offset((uint32_t)r, (uint32_t)(kbyte & 127));
 }
+
+// 64 rows x 64 K values of X, converted to the compute type, into smem.
+template <class T>
+__device__ __forceinline__ void load_tile64(const PackArgs &a, int64_t r0, int64_t k0, T (*tile)[65]) {
+  const int tid = threadIdx.x;
+#pragma unroll 4
+  for (int i = 0; i < 16; ++i) {
+    int e = tid + 256 * i, rr, kk;
+    if (a.rfast) { rr = e & 63; kk = e >> 6; } else { kk = e & 63; rr = e >> 6; }
+    int64_t r = r0 + rr, k = k0 + kk;
+    T v = (T)0;
+    if (r < a.rows && k < a.K) v = Loader<T>::load(a.X, a.Xbase + a.offR[r] + a.offK[k], a.TX, a.conj);
+    tile[rr][kk] = v;
+  }
+}
+
+// Ozaki slicing of 64 rows: pass 1 finds each row's max magnitude (and any
+// non-finite value), pass 2 writes s digit planes:
+//   x = v * 2^-e (|x| < 1); for p = 1..s: y = 128 x; d_p = trunc(y); x = y - d_p
+// so v = 2^e * (sum_p d_p 2^-7p + r 2^-7s) with |d_p| <= 127, all exact.
+__global__ void __launch_bounds__(256) oz_pack_kernel(PackArgs a) {
+  __shared__ double tile[64][65];
+  const int tid = threadIdx.x;
+  const int row = tid >> 2, part = tid & 3;
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  double amax = 0.0;
+  bool bad = false;
+  for (int64_t k0 = 0; k0 < a.K; k0 += 64) {
+    load_tile64<double>(a, r0, k0, tile);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      double v = tile[row][part * 16 + kk];
+      if (!isfinite(v)) bad = true;
+      amax = fmax(amax, fabs(v));
+    }
+    __syncthreads();
+  }
+  amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, 1));
+  amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, 2));
+  bad = __shfl_xor_sync(0xffffffffu, (int)bad, 1) || bad;
+  bad = __shfl_xor_sync(0xffffffffu, (int)bad, 2) || bad;
+  int e = 0;
+  if (bad) e = kNonFinite;
+  else if (amax > 0.0) frexp(amax, &e);
+  const int64_t grow = r0 + row;
+  if (part == 0 && grow < a.rows_pad) {
+    a.exp_out[grow] = e;
+    if (bad && grow < a.rows) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
+  }
+  const int64_t kpad = (int64_t)a.kblocks * kKBytes;
+  for (int64_t k0 = 0; k0 < kpad; k0 += 64) {
+    load_tile64<double>(a, r0, k0, tile);
+    __syncthreads();
+    if (grow < a.rows_pad) {
+      double x[16];
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk) {
+        double v = tile[row][part * 16 + kk];
+        x[kk] = (e == kNonFinite) ? 0.0 : ldexp(v, -e);
+      }
+      const int64_t off = panel_tile_base(a, grow, k0 + part * 16);
+      for (int p = 0; p < a.nslices; ++p) {
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+          double y = x[kk] * 128.0;
+          double d = trunc(y);
+          x[kk] = y - d;
+          uint32_t byte = (uint32_t)((int32_t)d) & 0xFFu;
+          w[kk >> 2] |= byte << (8 * (kk & 3));
+        }
+        *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Split-BF16 planes: hi = bf16(x), lo = bf16(x - hi), x in FP32.
+__global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
+  __shared__ float tile[64][65];
+  const int tid = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  const int64_t kpad = (int64_t)a.kblocks * (kKBytes / 2);  // elements
+  for (int64_t k0 = 0; k0 < kpad; k0 += 64) {
+    load_tile64<float>(a, r0, k0, tile);
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int item = tid + 256 * h;  // 64 rows x 8 chunks of 8 values
+      int row = item >> 3, c = item & 7;
+      int64_t grow = r0 + row;
+      if (grow < a.rows_pad) {
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float x0 = tile[row][c * 8 + 2 * q], x1 = tile[row][c * 8 + 2 * q + 1];
+          __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+          __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+          __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+          hw[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+          lw[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        }
+        const int64_t off = panel_tile_base(a, grow, (k0 + c * 8) * 2);
+        *reinterpret_cast<uint4 *>(a.panel + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4 *>(a.panel + a.plane + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- GEMM ---
+
+enum { KIND_I8 = 0, KIND_BF16 = 1 };
+
+struct GemmArgs {
+  const uint8_t *panelA, *panelB;
+  int64_t planeA, planeB;
+  int mtiles, ntiles, kblocks;
+  int nslices;       // Ozaki slices (I8)
+  int kseg_blocks;   // K blocks per INT32-exact segment (I8)
+  int nkseg;         // K segments per diagonal (I8)
+  const int32_t *expA, *expB;
+  void *C;
+  int64_t Cbase;
+  int TC;
+  const int64_t *offMC, *offNC;
+  int64_t M, N;
+  double alpha, beta;
+  int beta_case;
+  int *status;
+};
+
+template <int KIND>
+struct GemmCfg;
+template <>
+struct GemmCfg<KIND_I8> {
+  static constexpr int BN = 128, STAGES = 6, KSTEP_BYTES = 32;
+  static constexpr uint32_t IDESC = idesc_i8(128, 128);
+};
+template <>
+struct GemmCfg<KIND_BF16> {
+  static constexpr int BN = 256, STAGES = 4, KSTEP_BYTES = 32;
+  static constexpr uint32_t IDESC = idesc_bf16(128, 256);
+};
+
+template <int KIND>
+constexpr size_t gemm_smem_bytes() {
+  using Cfg = GemmCfg<KIND>;
+  return 1024 + (size_t)Cfg::STAGES * (kTileM * kKBytes + Cfg::BN * kKBytes) + 1024 +
+         Cfg::BN * (sizeof(int64_t) + sizeof(int32_t));
+}
+
+__device__ __forceinline__ int seg_count(const GemmArgs &a, int kind) {
+  return kind == KIND_I8 ? a.nslices * a.nkseg : 1;
+}
+// Terms of segment g: (plane of A, plane of B) for term index j, and the K
+// block range.
+__device__ __forceinline__ int seg_terms(const GemmArgs &a, int kind, int g) {
+  return kind == KIND_I8 ? (g / a.nkseg) + 1 : 3;
+}
+__device__ __forceinline__ void seg_term(const GemmArgs &a, int kind, int g, int j, int &pa, int &pb) {
+  if (kind == KIND_I8) {
+    int t = g / a.nkseg;
+    pa = j;
+    pb = t - j;
+  } else {
+    pa = (j == 2) ? 1 : 0;  // (hi,hi), (hi,lo), (lo,hi)
+    pb = (j == 1) ? 1 : 0;
+  }
+}
+__device__ __forceinline__ void seg_krange(const GemmArgs &a, int kind, int g, int &kb0, int &kb1) {
+  if (kind == KIND_I8) {
+    int ks = g % a.nkseg;
+    kb0 = ks * a.kseg_blocks;
+    kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
+  } else {
+    kb0 = 0;
+    kb1 = a.kblocks;
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ GemmArgs a) {
+  using Cfg = GemmCfg<KIND>;
+  constexpr int BN = Cfg::BN, STAGES = Cfg::STAGES;
+  constexpr uint32_t A_BYTES = kTileM * kKBytes, B_BYTES = BN * kKBytes;
+  constexpr int KSTEPS = kKBytes / Cfg::KSTEP_BYTES;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + STAGES * A_BYTES;
+  uint64_t *bars = (uint64_t *)(sB + STAGES * B_BYTES);
+  uint64_t *full = bars, *empty = bars + STAGES, *accf = bars + 2 * STAGES, *acce = accf + 2;
+  uint32_t *tmem_slot = (uint32_t *)(acce + 2);
+  volatile int *abort = (volatile int *)(tmem_slot + 1);
+  int64_t *s_offN = (int64_t *)(smem + STAGES * (A_BYTES + B_BYTES) + 1024);
+  int32_t *s_expN = (int32_t *)(s_offN + BN);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    *abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int ntile_total = a.mtiles * a.ntiles;
+  const int nseg = seg_count(a, KIND);
+
+  if (warp == 0) {
+    // ---------------------------------------------------- producer ----
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+        const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+        for (int g = 0; g < nseg; ++g) {
+          int kb0, kb1;
+          seg_krange(a, KIND, g, kb0, kb1);
+          const int nt_terms = seg_terms(a, KIND, g);
+          for (int j = 0; j < nt_terms; ++j) {
+            int pa, pb;
+            seg_term(a, KIND, g, j, pa, pb);
+            const uint8_t *srcA = a.panelA + pa * a.planeA + ((int64_t)mt * a.kblocks) * A_BYTES;
+            const uint8_t *srcB = a.panelB + pb * a.planeB + ((int64_t)nt * a.kblocks) * B_BYTES;
+            for (int kb = kb0; kb < kb1; ++kb) {
+              if (!mbar_wait(&empty[stage], phase ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+              mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
+              bulk_g2s(sA + stage * A_BYTES, srcA + (int64_t)kb * A_BYTES, A_BYTES, &full[stage]);
+              bulk_g2s(sB + stage * B_BYTES, srcB + (int64_t)kb * B_BYTES, B_BYTES, &full[stage]);
+              if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+              }
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------- MMA ------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0, sc = 0;
+      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+        for (int g = 0; g < nseg; ++g, ++sc) {
+          const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
+          if (!mbar_wait(&acce[buf], ap ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+          tc_fence_after();
+          const uint32_t d = tmem + buf * BN;
+          int kb0, kb1;
+          seg_krange(a, KIND, g, kb0, kb1);
+          const int nt_terms = seg_terms(a, KIND, g);
+          uint32_t acc = 0;
+          for (int j = 0; j < nt_terms; ++j) {
+            for (int kb = kb0; kb < kb1; ++kb) {
+              if (!mbar_wait(&full[stage], phase, abort, a.status, QS_ETIMEOUT)) goto done;
+              tc_fence_after();
+              const uint32_t a0 = smem_u32(sA + stage * A_BYTES), b0 = smem_u32(sB + stage * B_BYTES);
+#pragma unroll
+              for (int ks = 0; ks < KSTEPS; ++ks) {
+                const uint64_t ad = sw128_kmajor_desc(a0 + ks * Cfg::KSTEP_BYTES);
+                const uint64_t bd = sw128_kmajor_desc(b0 + ks * Cfg::KSTEP_BYTES);
+                if (KIND == KIND_I8) mma_i8(d, ad, bd, Cfg::IDESC, acc);
+                else mma_f16(d, ad, bd, Cfg::IDESC, acc);
+                acc = 1;
+              }
+              tc_commit(&empty[stage]);
+              if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1;
+              }
+            }
+          }
+          tc_commit(&accf[buf]);
+        }
+      }
+    }
+  } else {
+    // --------------------------------------------------- epilogue -----
+    const int q = warp & 3;           // TMEM lane quarter of this warp
+    const int et = threadIdx.x - 64;  // 0..127
+    const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+    uint32_t sc = 0;
+    for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+      const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+      const int64_t m0 = (int64_t)mt * kTileM, n0 = (int64_t)nt * BN;
+      named_bar_sync(1, 128);
+      for (int j = et; j < BN; j += 128) {
+        int64_t n = n0 + j;
+        s_offN[j] = n < a.N ? a.offNC[n] : 0;
+        s_expN[j] = (KIND == KIND_I8 && n < a.N) ? a.expB[n] : 0;
+      }
+      named_bar_sync(1, 128);
+      const int64_t i = m0 + 32 * q + lane;
+      const bool row_ok = i < a.M;
+      const int eA = (KIND == KIND_I8 && row_ok) ? a.expA[i] : 0;
+      const int64_t crow = row_ok ? a.Cbase + a.offMC[i] : 0;
+      const bool row_store = row_ok && eA != kNonFinite;
+      for (int g = 0; g < nseg; ++g, ++sc) {
+        const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
+        if (!mbar_wait(&accf[buf], ap, abort, a.status, QS_ETIMEOUT)) goto done;
+        tc_fence_after();
+        const bool first = (g == 0), last = (g == nseg - 1);
+        const uint32_t tacc = tmem + lane_base + buf * BN;
+        const uint32_t tsum = tmem + lane_base + 256;
+        double w = 1.0;
+        if (KIND == KIND_I8) w = ldexp(1.0, -7 * ((g / a.nkseg) + 2));
+#pragma unroll 1
+        for (int c = 0; c < BN / 16; ++c) {
+          uint32_t dr[16], sr[32];
+          tmem_ld16(tacc + 16 * c, dr);
+          if (KIND == KIND_I8 && !first) {
+            tmem_ld16(tsum + 32 * c, sr);
+            tmem_ld16(tsum + 32 * c + 16, sr + 16);
+          }
+          tmem_ld_wait();
+          if (KIND == KIND_I8) {
+            double v[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              double s0 = first ? 0.0 : __hiloint2double((int)sr[2 * e + 1], (int)sr[2 * e]);
+              v[e] = fma((double)(int32_t)dr[e], w, s0);
+            }
+            if (!last) {
+#pragma unroll
+              for (int e = 0; e < 16; ++e) {
+                sr[2 * e] = (uint32_t)__double2loint(v[e]);
+                sr[2 * e + 1] = (uint32_t)__double2hiint(v[e]);
+              }
+              tmem_st16(tsum + 32 * c, sr);
+              tmem_st16(tsum + 32 * c + 16, sr + 16);
+            } else if (row_store) {
+#pragma unroll 4
+              for (int e = 0; e < 16; ++e) {
+                const int jj = 16 * c + e;
+                const int64_t n = n0 + jj;
+                const int eB = s_expN[jj];
+                if (n < a.N && eB != kNonFinite) {
+                  const double val = ldexp(v[e], eA + eB);
+                  const int64_t idx = crow + s_offN[jj];
+                  double out;
+                  if (a.beta_case == 0) out = a.alpha * val;
+                  else {
+                    const double old = load_c<double>(a.C, idx, a.TC);
+                    out = a.beta_case == 1 ? fma(a.alpha, val, old) : fma(a.alpha, val, a.beta * old);
+                  }
+                  store_c<double>(a.C, idx, a.TC, out);
+                }
+              }
+            }
+          } else if (row_ok) {
+            const float al = (float)a.alpha, be = (float)a.beta;
+#pragma unroll 4
+            for (int e = 0; e < 16; ++e) {
+              const int jj = 16 * c + e;
+              const int64_t n = n0 + jj;
+              if (n < a.N) {
+                const float val = __uint_as_float(dr[e]);
+                const int64_t idx = crow + s_offN[jj];
+                float out;
+                if (a.beta_case == 0) out = al * val;
+                else {
+                  const float old = load_c<float>(a.C, idx, a.TC);
+                  out = a.beta_case == 1 ? fmaf(al, val, old) : fmaf(al, val, be * old);
+                }
+                store_c<float>(a.C, idx, a.TC, out);
+              }
+            }
+          }
+        }
+        if (KIND == KIND_I8 && !last) tmem_st_wait();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acce[buf]);
+      }
+    }
+  }
+done:
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort) {
+    // Give in-flight copies and MMAs time to land before TMEM is released.
+    const uint64_t t0 = globaltimer_ns();
+    while (globaltimer_ns() - t0 < 2000000ull) {
+    }
+  }
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// Non-finite rows of A / columns of B (flagged by the pack): those elements
+// of C are computed here directly in FP64 (IEEE semantics), and the GEMM's
+// epilogue skipped them.
+__global__ void oz_fixup_kernel(Operands op, double alpha, double beta, int beta_case,
+                                const int32_t *rows, const int32_t *nrows, const int32_t *cols,
+                                const int32_t *ncols, const int32_t *expA) {
+  const int nr = *nrows, nc = *ncols;
+  const int64_t total = (int64_t)nr * op.N + (int64_t)nc * op.M;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j;
+    if (e < (int64_t)nr * op.N) {
+      i = rows[e / op.N];
+      j = e % op.N;
+    } else {
+      int64_t f = e - (int64_t)nr * op.N;
+      j = cols[f / op.M];
+      i = f % op.M;
+      if (expA[i] == kNonFinite) continue;  // done by the row pass
+    }
+    double acc = 0.0;
+    for (int64_t k = 0; k < op.K; ++k) {
+      double x = Loader<double>::load(op.A, op.Abase + op.offMA[i] + op.offKA[k], op.TA, op.conjA);
+      double y = Loader<double>::load(op.B, op.Bbase + op.offNB[j] + op.offKB[k], op.TB, op.conjB);
+      acc = fma(x, y, acc);
+    }
+    const int64_t idx = op.Cbase + op.offMC[i] + op.offNC[j];
+    double out;
+    if (beta_case == 0) out = alpha * acc;
+    else {
+      double old = load_c<double>(op.C, idx, op.TC);
+      out = beta_case == 1 ? fma(alpha, acc, old) : fma(alpha, acc, beta * old);
+    }
+    store_c<double>(op.C, idx, op.TC, out);
+  }
+}
+
+// ------------------------------------------------------------- host side ---
+
+static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+int tc_auto_method(const qs_plan *p) {
+  // The tensor-core paths pay a pack pass and pad to 128-row tiles: worth it
+  // once every extent fills a tile.  Complex plans stay on the gather kernel
+  // until the 1m epilogue lands.
+  if (is_complex(p->T)) return QS_METHOD_NATIVE;
+  if (p->M < 128 || p->N < 128 || p->K < 64) return QS_METHOD_NATIVE;
+  return is_double(p->T) ? QS_METHOD_OZAKI_I8 : QS_METHOD_BF16X3;
+}
+
+static int default_slices(int64_t K) {
+  // 7 signed 7-bit slices (28 slice products) reach ~1e-14 relative
+  // Frobenius error at K = 2304 on uniform and 2^+-20-scaled inputs; longer
+  // K gets one more slice per 16x of K (the error grows like sqrt(K)).
+  int s = 7;
+  if (K > 16384) s = 8;
+  return s;
+}
+
+void tc_geometry(qs_plan *p) {
+  TensorCoreGeom &g = p->tc;
+  g = TensorCoreGeom{};
+  if (p->method == QS_METHOD_OZAKI_I8) {
+    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(p->K);
+    p->ozaki_slices = g.nslices;
+    g.kblocks = cdiv(p->K, 128);
+    g.mtiles = cdiv(p->M, 128);
+    g.ntiles = cdiv(p->N, 128);
+    g.Mp = g.mtiles * 128;
+    g.Np = g.ntiles * 128;
+    g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
+    g.plane_bytes_b = g.ntiles * g.kblocks * 128 * 128;
+    // INT32-exact segment: (terms) * kblocks * 128 * 127^2 < 2^31.
+    int64_t maxkb = (int64_t)(2147483647ll / ((int64_t)g.nslices * 128 * 127 * 127));
+    if (maxkb < 1) maxkb = 1;
+    g.kseg = (int)std::min<int64_t>(maxkb, g.kblocks);
+  } else {
+    g.nslices = 2;
+    g.kblocks = cdiv(p->K, 64);
+    g.mtiles = cdiv(p->M, 128);
+    g.ntiles = cdiv(p->N, 256);
+    g.Mp = g.mtiles * 128;
+    g.Np = g.ntiles * 256;
+    g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
+    g.plane_bytes_b = g.ntiles * g.kblocks * 256 * 128;
+    g.kseg = (int)g.kblocks;
+  }
+}
+
+static int tc_alloc(qs_plan *p, void **out, size_t bytes) {
+  *out = nullptr;
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    std::ostringstream s;
+    s << "device allocation of " << bytes << " bytes failed: " << cudaGetErrorString(e);
+    return fail(QS_ENOMEM, s.str());
+  }
+  p->ws.owned.push_back(*out);
+  p->ws.bytes += bytes;
+  return QS_OK;
+}
+
+int tc_prepare(qs_plan *p) {
+  tc_geometry(p);
+  const TensorCoreGeom &g = p->tc;
+  int rc;
+  void *q;
+  if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_a * g.nslices))) return rc;
+  p->ws.panelA = q;
+  if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_b * g.nslices))) return rc;
+  p->ws.panelB = q;
+  if (p->method == QS_METHOD_OZAKI_I8) {
+    // exponents (padded rows/cols), non-finite lists, their counters, status
+    size_t n = (size_t)(g.Mp + g.Np + p->M + p->N + 4);
+    if ((rc = tc_alloc(p, &q, n * sizeof(int32_t)))) return rc;
+    int32_t *b = (int32_t *)q;
+    p->ws.expA = b;
+    p->ws.expB = b + g.Mp;
+    if (cudaMemset(q, 0, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
+    p->ws.status = b + n - 1;
+  } else {
+    if ((rc = tc_alloc(p, &q, 4 * sizeof(int32_t)))) return rc;
+    if (cudaMemset(q, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
+    p->ws.status = (int32_t *)q;
+  }
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[0]) {
+    cudaFuncSetAttribute(tc_gemm_kernel<KIND_I8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)gemm_smem_bytes<KIND_I8>());
+    cudaFuncSetAttribute(tc_gemm_kernel<KIND_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)gemm_smem_bytes<KIND_BF16>());
+    attr_set[0] = attr_set[1] = true;
+  }
+  return QS_OK;
+}
+
+static int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+static PackArgs pack_args(const qs_plan *p, int side) {
+  const TensorCoreGeom &g = p->tc;
+  PackArgs a;
+  if (side == 0) {
+    a.X = p->Adata; a.Xbase = p->Abase; a.TX = p->TA; a.conj = p->conjA;
+    a.offR = p->ws.offM[0]; a.offK = p->ws.offK[0];
+    a.rows = p->M; a.rows_pad = g.Mp; a.tile_rows = 128;
+    a.rfast = p->a_mfast;
+    a.panel = (uint8_t *)p->ws.panelA; a.plane = g.plane_bytes_a;
+    a.exp_out = p->ws.expA;
+  } else {
+    a.X = p->Bdata; a.Xbase = p->Bbase; a.TX = p->TB; a.conj = p->conjB;
+    a.offR = p->ws.offN[0]; a.offK = p->ws.offK[1];
+    a.rows = p->N; a.rows_pad = g.Np; a.tile_rows = p->method == QS_METHOD_BF16X3 ? 256 : 128;
+    a.rfast = p->b_nfast;
+    a.panel = (uint8_t *)p->ws.panelB; a.plane = g.plane_bytes_b;
+    a.exp_out = p->ws.expB;
+  }
+  a.K = p->K;
+  a.kblocks = (int)g.kblocks;
+  a.nslices = g.nslices;
+  if (p->method == QS_METHOD_OZAKI_I8) {
+    int32_t *lists = p->ws.expA + g.Mp + g.Np;
+    int32_t *counters = lists + p->M + p->N;
+    a.flag_list = side == 0 ? lists : lists + p->M;
+    a.flag_count = counters + side;
+  } else {
+    a.flag_list = a.flag_count = nullptr;
+    a.exp_out = nullptr;
+  }
+  return a;
+}
+
+int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
+               cudaStream_t st) {
+  const TensorCoreGeom &g = p->tc;
+  const bool oz = p->method == QS_METHOD_OZAKI_I8;
+  int launches = 0;
+  cudaError_t e;
+  if (oz) {
+    int32_t *counters = p->ws.expA + g.Mp + g.Np + p->M + p->N;
+    e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
+    if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
+  }
+  for (int side = 0; side < 2; ++side) {
+    PackArgs pa = pack_args(p, side);
+    dim3 grid((unsigned)cdiv(pa.rows_pad, 64));
+    if (oz) oz_pack_kernel<<<grid, 256, 0, st>>>(pa);
+    else bf16_pack_kernel<<<grid, 256, 0, st>>>(pa);
+    ++launches;
+  }
+  GemmArgs a;
+  a.panelA = (const uint8_t *)p->ws.panelA;
+  a.panelB = (const uint8_t *)p->ws.panelB;
+  a.planeA = g.plane_bytes_a;
+  a.planeB = g.plane_bytes_b;
+  a.mtiles = (int)g.mtiles;
+  a.ntiles = (int)g.ntiles;
+  a.kblocks = (int)g.kblocks;
+  a.nslices = g.nslices;
+  a.kseg_blocks = oz ? g.kseg : (int)g.kblocks;
+  a.nkseg = oz ? (int)cdiv(g.kblocks, g.kseg) : 1;
+  a.expA = p->ws.expA;
+  a.expB = p->ws.expB;
+  a.C = p->Cdata;
+  a.Cbase = p->Cbase;
+  a.TC = p->TC;
+  a.offMC = p->ws.offM[1];
+  a.offNC = p->ws.offN[1];
+  a.M = p->M;
+  a.N = p->N;
+  a.alpha = alpha[0];
+  a.beta = beta[0];
+  a.beta_case = beta_case;
+  a.status = p->ws.status;
+  const int tiles = a.mtiles * a.ntiles;
+  const int grid = std::min(tiles, num_sms());
+  if (oz) {
+    tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+  } else {
+    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a);
+  }
+  ++launches;
+  if (oz) {
+    Operands op;
+    op.A = p->Adata; op.B = p->Bdata; op.C = p->Cdata;
+    op.Abase = p->Abase; op.Bbase = p->Bbase; op.Cbase = p->Cbase;
+    op.TA = p->TA; op.TB = p->TB; op.TC = p->TC;
+    op.conjA = p->conjA; op.conjB = p->conjB;
+    op.offMA = p->ws.offM[0]; op.offMC = p->ws.offM[1];
+    op.offNB = p->ws.offN[0]; op.offNC = p->ws.offN[1];
+    op.offKA = p->ws.offK[0]; op.offKB = p->ws.offK[1];
+    op.M = p->M; op.N = p->N; op.K = p->K;
+    int32_t *lists = p->ws.expA + g.Mp + g.Np;
+    int32_t *counters = lists + p->M + p->N;
+    oz_fixup_kernel<<<64, 256, 0, st>>>(op, alpha[0], beta[0], beta_case, lists, counters,
+                                        lists + p->M, counters + 1, p->ws.expA);
+    ++launches;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::ostringstream s;
+    s << "CUDA error in tensor-core launch: " << cudaGetErrorString(e);
+    return fail(QS_ECUDA, s.str());
+  }
+  count_launches(launches);
+  return QS_OK;
+}
+
 int tc_execute_grouped(int n, qs_plan *const *plans, const double *alpha, const double *beta,
                        cudaStream_t st) {
   for (int i = 0; i < n; ++i) {

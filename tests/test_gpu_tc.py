@@ -1,0 +1,170 @@
+"""GPU parity of the tensor-core paths: Float64 through INT8 Ozaki slices
+(tcgen05 kind::i8) and Float32 through split-BF16 x3 (kind::f16), against the
+oracle evaluated in binary128.  Tolerances are the stated targets:
+relative Frobenius error <= 1e-13 (Float64), <= 1e-5 (Float32).
+"""
+import numpy as np
+import pytest
+import torch
+
+from _util import Pair, colmajor_pair, rel_fro, run_pair
+
+pytestmark = pytest.mark.gpu
+TOL64, TOL32 = 1e-13, 1e-5
+
+
+def uniform_pair(qs, rng, shape, et="Float64", scale_axis=None):
+    n = int(np.prod(shape))
+    v = rng.uniform(-1.0, 1.0, n)
+    if scale_axis is not None:
+        arr = v.reshape(shape, order="F")
+        u = np.exp2(rng.integers(-20, 21, shape[scale_axis]).astype(np.float64))
+        sh = [1] * len(shape)
+        sh[scale_axis] = shape[scale_axis]
+        v = (arr * u.reshape(sh)).ravel(order="F")
+    st, acc = [], 1
+    for s in shape:
+        st.append(acc)
+        acc *= s
+    return Pair(qs, v.astype(np.float64 if et == "Float64" else np.float32), tuple(shape), tuple(st))
+
+
+@pytest.mark.parametrize("MKN", [(256, 300, 384), (200, 333, 130), (128, 64, 128), (1000, 129, 777)])
+@pytest.mark.parametrize("beta", [0.0, 1.0, 0.7])
+def test_ozaki_matmul_matches_oracle(qs, orc, MKN, beta):
+    M, K, N = MKN
+    rng = np.random.default_rng(M * 7 + K)
+    A = uniform_pair(qs, rng, (M, K))
+    B = uniform_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "Float64", fill=np.nan if beta == 0 else None)
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), beta, (1, 3), method="ozaki",
+                              precision=1)
+    assert plan.method == "ozaki" and plan.ozaki_slices >= 7
+    assert np.all(np.isfinite(got))
+    assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+def test_ozaki_is_the_default_for_float64(qs):
+    rng = np.random.default_rng(0)
+    A = uniform_pair(qs, rng, (256, 256))
+    B = uniform_pair(qs, rng, (256, 256))
+    C = colmajor_pair(qs, rng, (256, 256), "Float64")
+    assert qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3)).method == "ozaki"
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_ozaki_permuted_4index(qs, orc, wide):
+    # C[a,b,c,d] = sum_{e,f} A[a,e,b,f] * B[f,c,e,d] at a=b=c=d=32, e=f=24,
+    # with the wide-exponent distribution scaling A along a and B along d.
+    rng = np.random.default_rng(5 + wide)
+    A = uniform_pair(qs, rng, (32, 24, 32, 24), scale_axis=0 if wide else None)
+    B = uniform_pair(qs, rng, (24, 32, 24, 32), scale_axis=3 if wide else None)
+    C = colmajor_pair(qs, rng, (32, 32, 32, 32), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 5, 2, 6), B, (6, 3, 5, 4), 0.7, (1, 2, 3, 4),
+                              method="ozaki", precision=1)
+    assert plan.method == "ozaki"
+    assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+def test_ozaki_persistent_tiles_and_reuse(qs, orc):
+    # 16 x 16 = 256 tiles > SM count: every CTA runs more than one tile.
+    rng = np.random.default_rng(9)
+    M = N = 2048
+    K = 256
+    A = uniform_pair(qs, rng, (M, K))
+    B = uniform_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "Float64", fill=0.0)
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3), method="ozaki")
+    qs.execute(plan, 1.0, 0.0)
+    first = C.device_parent().copy()
+    sample = (0, 4 * M + 17)
+    orc.brute(C.host, 1.0, A.host, (1, 2), B.host, (2, 3), 0.0, (1, 3), c_range=sample, precision=1)
+    assert rel_fro(first[:sample[1]], C.host.parent[:sample[1]]) <= TOL64
+    # last columns (last tiles of the schedule)
+    lo = (N - 3) * M
+    orc.brute(C.host, 1.0, A.host, (1, 2), B.host, (2, 3), 0.0, (1, 3), c_range=(lo, N * M), precision=1)
+    assert rel_fro(first[lo:], C.host.parent[lo:]) <= TOL64
+    C.dev.parent.fill_(float("nan"))
+    qs.execute(plan, 1.0, 0.0)
+    assert np.array_equal(C.device_parent(), first)
+
+
+def test_ozaki_long_k_segments(qs, orc):
+    # K beyond one INT32-exact segment (148 K blocks at 7 slices).
+    rng = np.random.default_rng(10)
+    M, K, N = 128, 20000, 128
+    A = uniform_pair(qs, rng, (M, K))
+    B = uniform_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), method="ozaki",
+                              ozaki_slices=7, precision=1)
+    assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+def test_ozaki_nonfinite_rows_and_columns(qs, orc):
+    # NaN/Inf in a row of A or a column of B: those elements are computed
+    # with IEEE semantics like the reference's loops; the rest stay exact.
+    rng = np.random.default_rng(11)
+    M, K, N = 256, 128, 200
+    a = rng.uniform(-1, 1, (M, K))
+    b = rng.uniform(-1, 1, (K, N))
+    a[3, 5] = np.nan
+    a[100, 0] = np.inf
+    b[7, 150] = -np.inf
+    A = Pair(qs, a.ravel(order="F"), (M, K), (1, M))
+    B = Pair(qs, b.ravel(order="F"), (K, N), (1, K))
+    C = colmajor_pair(qs, rng, (M, N), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), method="ozaki",
+                              precision=1)
+    g = got.reshape(N, M).T
+    r = ref.reshape(N, M).T
+    assert np.array_equal(np.isnan(g), np.isnan(r))
+    assert np.array_equal(np.isinf(g), np.isinf(r))
+    fin = np.isfinite(r)
+    assert np.all(g[fin] == g[fin])
+    assert rel_fro(g[fin], r[fin]) <= TOL64
+
+
+def test_ozaki_mixed_input_eltypes(qs, orc):
+    # Float32 A with Float64 B and C: compute type Float64, conversion on load.
+    rng = np.random.default_rng(12)
+    A = uniform_pair(qs, rng, (300, 200), et="Float32")
+    B = uniform_pair(qs, rng, (200, 260))
+    C = colmajor_pair(qs, rng, (300, 260), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1)
+    assert plan.method == "ozaki"
+    assert rel_fro(got, ref) <= TOL64
+
+
+@pytest.mark.parametrize("MKN", [(256, 256, 256), (300, 200, 520), (1024, 512, 1024)])
+def test_bf16x3_float32_matches_oracle(qs, orc, MKN):
+    M, K, N = MKN
+    rng = np.random.default_rng(M + N)
+    A = uniform_pair(qs, rng, (M, K), et="Float32")
+    B = uniform_pair(qs, rng, (K, N), et="Float32")
+    C = colmajor_pair(qs, rng, (M, N), "Float32")
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3))
+    assert plan.method == "bf16x3"
+    qs.execute(plan, 1.5, 0.5)
+    got = C.device_parent()
+    # FP64 oracle on the same Float32 inputs
+    Ch = orc.HostView(C.host.parent.astype(np.float64), C.host.size, C.host.strides)
+    Ah = orc.HostView(A.host.parent.astype(np.float64), A.host.size, A.host.strides)
+    Bh = orc.HostView(B.host.parent.astype(np.float64), B.host.size, B.host.strides)
+    orc.brute(Ch, 1.5, Ah, (1, 2), Bh, (2, 3), 0.5, (1, 3))
+    assert rel_fro(got.astype(np.float64), Ch.parent) <= TOL32, rel_fro(got.astype(np.float64), Ch.parent)
+
+
+def test_bf16x3_wide_exponents(qs, orc):
+    rng = np.random.default_rng(13)
+    A = uniform_pair(qs, rng, (256, 300), et="Float32", scale_axis=0)
+    B = uniform_pair(qs, rng, (300, 384), et="Float32", scale_axis=1)
+    C = colmajor_pair(qs, rng, (256, 384), "Float32", fill=np.nan)
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3))
+    qs.execute(plan, 1.0, 0.0)
+    got = C.device_parent().astype(np.float64)
+    Ch = orc.HostView(np.zeros(256 * 384), (256, 384), (1, 256))
+    Ah = orc.HostView(A.host.parent.astype(np.float64), A.host.size, A.host.strides)
+    Bh = orc.HostView(B.host.parent.astype(np.float64), B.host.size, B.host.strides)
+    orc.brute(Ch, 1.0, Ah, (1, 2), Bh, (2, 3), 0.0, (1, 3))
+    assert rel_fro(got, Ch.parent) <= TOL32
