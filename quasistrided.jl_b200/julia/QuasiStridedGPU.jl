@@ -1,0 +1,184 @@
+# QuasiStridedGPU — Julia binding of libqsgpu.so (include/qsgpu.h).
+#
+# Device-resident strided operands drop into QuasiStrided's API: the labels
+# are resolved by the library's planner (the same rules as
+# src/planning/labels.jl), and execution runs on the B200 kernels.  Shipped
+# as source; it needs CUDA.jl for device arrays and streams.
+module QuasiStridedGPU
+
+using CUDA
+import TensorOperations as TO
+
+const libqsgpu = get(ENV, "QSGPU_LIB", joinpath(@__DIR__, "..", "lib", "libqsgpu.so"))
+
+# --- C structs (layout of include/qsgpu.h) ---------------------------------
+
+struct QSView
+    data::Ptr{Cvoid}
+    length::Int64
+    offset::Int64
+    size::Ptr{Int64}
+    strides::Ptr{Int64}
+    ndim::Int32
+    eltype::Int32
+    op::Int32
+    reserved::Int32
+end
+
+Base.@kwdef struct QSPlanOptions
+    conjA::Int32 = 0
+    conjB::Int32 = 0
+    accumulator::Int32 = 0
+    method::Int32 = 0
+    m_block::Int64 = 0
+    k_block::Int64 = 0
+    n_block::Int64 = 0
+    dot_mode::Int32 = 0
+    outer_mode::Int32 = 0
+    unpacked_b_mode::Int32 = 0
+    ozaki_slices::Int32 = 0
+    complex_mode::Int32 = 0
+    flags::Int32 = 0
+end
+
+const ELTYPE = Dict(Float32 => Int32(0), Float64 => Int32(1), ComplexF32 => Int32(2), ComplexF64 => Int32(3))
+opcode(::typeof(identity)) = Int32(0)
+opcode(::typeof(conj)) = Int32(1)
+opcode(::typeof(transpose)) = Int32(2)
+opcode(::typeof(adjoint)) = Int32(3)
+opcode(f) = throw(ArgumentError("unsupported StridedView.op $f"))
+accode(::Nothing) = Int32(0)
+accode(::Type{Float32}) = Int32(1)
+accode(::Type{Float64}) = Int32(2)
+
+"""
+    DeviceStridedView(parent::CuArray, size, strides, offset, op = identity)
+
+A StridedView over device memory: the fields StridedViews.jl's `StridedView`
+carries (size, strides, offset, op) over a `CuArray` parent.
+"""
+struct DeviceStridedView{T, N, A <: CuArray{T}, F}
+    parent::A
+    size::NTuple{N, Int}
+    strides::NTuple{N, Int}
+    offset::Int
+    op::F
+end
+DeviceStridedView(a::CuArray{T, N}) where {T, N} =
+    DeviceStridedView(a, size(a), strides(a), 0, identity)
+Base.eltype(::DeviceStridedView{T}) where {T} = T
+
+function check(rc::Cint)
+    rc == 0 && return nothing
+    buf = Vector{UInt8}(undef, 4096)
+    ccall((:qs_last_error, libqsgpu), Csize_t, (Ptr{UInt8}, Csize_t), buf, length(buf))
+    msg = unsafe_string(pointer(buf))
+    rc == 1 && throw(ArgumentError(msg))
+    rc == 2 && throw(DimensionMismatch(msg))
+    rc == 3 && throw(BoundsError(msg))
+    rc == 7 && throw(ArgumentError(msg))
+    error("qsgpu status $rc: $msg")
+end
+
+# Build the C view; the size/stride vectors are kept alive by the caller.
+function cview(v::DeviceStridedView{T}, keep) where {T}
+    sz = collect(Int64, v.size)
+    st = collect(Int64, v.strides)
+    push!(keep, sz, st)
+    return QSView(reinterpret(Ptr{Cvoid}, pointer(v.parent)), length(v.parent), v.offset,
+        pointer(sz), pointer(st), Int32(length(v.size)), ELTYPE[T], opcode(v.op), Int32(0))
+end
+
+mutable struct ContractPlan
+    handle::Ptr{Cvoid}
+    C::DeviceStridedView
+    A::DeviceStridedView
+    B::DeviceStridedView
+end
+
+release!(p::ContractPlan) = (p.handle != C_NULL && ccall((:qs_plan_destroy, libqsgpu), Cint, (Ptr{Cvoid},), p.handle); p.handle = C_NULL; nothing)
+
+"""
+    plan_contract(C, A, indA, B, indB, indC; conjA=false, conjB=false, accumulator=nothing)
+
+QuasiStrided.plan_contract for device views (src/planning/plan.jl:115-133).
+"""
+function plan_contract(C::DeviceStridedView, A::DeviceStridedView, indA::NTuple{NA, Int},
+        B::DeviceStridedView, indB::NTuple{NB, Int}, indC::NTuple{NC, Int};
+        conjA::Bool = false, conjB::Bool = false, accumulator = nothing) where {NA, NB, NC}
+    keep = Any[]
+    cC, cA, cB = cview(C, keep), cview(A, keep), cview(B, keep)
+    opts = QSPlanOptions(; conjA = Int32(conjA), conjB = Int32(conjB), accumulator = accode(accumulator))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve keep begin
+        check(ccall((:qs_plan_contract, libqsgpu), Cint,
+            (Ref{Ptr{Cvoid}}, Ref{QSView}, Ref{QSView}, Ptr{Int64}, Ref{QSView}, Ptr{Int64}, Ptr{Int64}, Ref{QSPlanOptions}),
+            h, cC, cA, collect(Int64, indA), cB, collect(Int64, indB), collect(Int64, indC), opts))
+    end
+    p = ContractPlan(h[], C, A, B)
+    finalizer(release!, p)
+    return p
+end
+
+"""
+    execute!(plan, alpha, beta) -> parent(C)
+
+QuasiStrided.execute! (src/execution/execute.jl:191): enqueued on CUDA.jl's
+current stream.
+"""
+function execute!(p::ContractPlan, alpha::Number, beta::Number)
+    a = Float64[real(alpha), imag(alpha)]
+    b = Float64[real(beta), imag(beta)]
+    stream = CUDA.stream().handle
+    check(ccall((:qs_execute, libqsgpu), Cint, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Cvoid}),
+        p.handle, a, b, reinterpret(Ptr{Cvoid}, stream)))
+    return p.C.parent
+end
+
+"""
+    contract!(C, alpha, A, indA, B, indB, beta, indC; accumulator = nothing) -> C
+"""
+function contract!(C::DeviceStridedView, alpha::Number, A::DeviceStridedView, indA, B::DeviceStridedView,
+        indB, beta::Number, indC; accumulator = nothing)
+    p = plan_contract(C, A, indA, B, indB, indC; accumulator)
+    execute!(p, alpha, beta)
+    CUDA.synchronize()
+    release!(p)
+    return C
+end
+
+"""
+    QuasiStridedGPUBackend(; accumulator = nothing)
+
+The device counterpart of QuasiStridedBackend
+(src/integrations/tensoroperations.jl:299-307).
+"""
+struct QuasiStridedGPUBackend{A} <: TO.AbstractBackend
+    function QuasiStridedGPUBackend{A}() where {A}
+        A in (nothing, Float32, Float64) ||
+            throw(ArgumentError("QuasiStridedGPUBackend: accumulator must be nothing, Float32 or Float64, got $A"))
+        return new{A}()
+    end
+end
+QuasiStridedGPUBackend(; accumulator = nothing) = QuasiStridedGPUBackend{accumulator}()
+
+function TO.tensorcontract!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::Bool,
+        B::CuArray, pB::TO.Index2Tuple, conjB::Bool, pAB::TO.Index2Tuple,
+        α::Number, β::Number, ::QuasiStridedGPUBackend{AC}, allocator = TO.DefaultAllocator()) where {AC}
+    NoA, Nk, NoB = length(pA[1]), length(pA[2]), length(pB[2])
+    lin(p) = Int64[p[1]..., p[2]...]
+    indA = Vector{Int64}(undef, NoA + Nk)
+    indB = Vector{Int64}(undef, Nk + NoB)
+    indC = Vector{Int64}(undef, NoA + NoB)
+    check(ccall((:qs_contraction_labels, libqsgpu), Cint,
+        (Int32, Int32, Int32, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}),
+        NoA, Nk, NoB, lin(pA), lin(pB), lin(pAB), indA, indB, indC))
+    p = plan_contract(DeviceStridedView(C), DeviceStridedView(A), Tuple(indA), DeviceStridedView(B),
+        Tuple(indB), Tuple(indC); conjA, conjB, accumulator = AC)
+    execute!(p, α, β)
+    CUDA.synchronize()
+    release!(p)
+    return C
+end
+
+end # module
