@@ -190,6 +190,23 @@ int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB,
 int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha,
                        const double *beta, void *stream);
 
+/* contract! without any device allocation.  No counterpart in the reference:
+ * it is for callers that cannot allocate device memory when they contract,
+ * e.g. a serving loop where cudaMalloc/cudaFree would synchronize the device
+ * and stall other in-flight work, or a host whose memory pool forbids raw
+ * allocations.  It plans on the host and runs the gather kernels with their
+ * M/N/K offset tables in one fixed-size file-scope device array, so it needs
+ * 2*(M+N+K) <= 524288 (QS_EINVAL otherwise) and does not use the
+ * tensor-core paths.  All calls share that array: calls that overlap on the
+ * GPU race.  The first call on a device looks the array up and should come
+ * before any stream capture on that device.  Arguments as qs_contract;
+ * returns once the work is enqueued on `stream`. */
+int qs_contract_noalloc(const qs_view *C, const double *alpha, const qs_view *A,
+                        const int64_t *indA, const qs_view *B,
+                        const int64_t *indB, const double *beta,
+                        const int64_t *indC, const qs_plan_options *opts,
+                        void *stream);
+
 /* Number of device kernels this library has launched in this process
  * (instrumentation: benchmarks difference it around a timed region). */
 int64_t qs_launch_count(void);

@@ -111,6 +111,9 @@ SIGNATURES = {
     "qs_execute_grouped": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P), _DP, _DP, _P]),
     "qs_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
     "qs_launch_count": (ctypes.c_int64, []),
+    "qs_contract_noalloc": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
+                                           ctypes.POINTER(qs_view), _I64P, _DP, _I64P,
+                                           ctypes.POINTER(qs_plan_options), _P]),
     "qs_version": (ctypes.c_char_p, []),
 }
 
