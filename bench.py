@@ -95,7 +95,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -139,6 +139,115 @@ def measured_peaks():
             return json.load(f), "measured"
     except OSError:
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+STAGE_NAMES = {"ozaki": ["pack_A", "pack_B", "gemm_i8", "fixup"],
+               "bf16x3": ["pack_A", "pack_B", "gemm_bf16"],
+               "native": ["gemm_native"]}
+
+
+def load_ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def roofline(plan, stage_ms, nexec):
+    """Roofline of the dominant kernel from the per-stage CUDA-event times of
+    the timed region.  Ozaki GEMM: algorithmic work = the slice products,
+    s(s+1)/2 * 2MNK int8 ops; peak = 2x the measured dense bf16 figure (the
+    B200's int8:bf16 dense ratio; no int8 figure is measured by the driver).
+    Native GEMM: 2MNK fp64 flops against the B200's nominal 40 TFLOP/s FP64."""
+    peaks, kind = measured_peaks()
+    names = STAGE_NAMES.get(plan.method, [f"stage{i}" for i in range(len(stage_ms))])
+    per = {names[i] if i < len(names) else f"stage{i}": stage_ms[i] / max(nexec, 1)
+           for i in range(len(stage_ms))}
+    if plan.method == "ozaki":
+        s = plan.ozaki_slices
+        work = s * (s + 1) / 2 * FLOPS
+        ms = per.get("gemm_i8")
+        peak = 2.0 * peaks["bf16_tflops"]
+        note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
+        kernel = "tc_gemm_kernel<KIND_I8>"
+    elif plan.method == "bf16x3":
+        work = 3 * FLOPS
+        ms = per.get("gemm_bf16")
+        peak = peaks["bf16_tflops"]
+        note = f"{kind} bf16 dense"
+        kernel = "tc_gemm_kernel<KIND_BF16>"
+    else:
+        work = FLOPS
+        ms = per.get("gemm_native")
+        peak = 40.0
+        note = "nominal B200 FP64 (no measured FP64 figure)"
+        kernel = "direct_gemm_kernel"
+    achieved = work / (ms * 1e-3) / 1e12 if ms else None
+    roof = {"bound": "tensor", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None, "traffic": load_ncu_traffic(kernel),
+            "ms_per_launch": ms, "peak_note": note}
+    return roof, per
+
+
+def measure_library_peaks():
+    """cuBLAS int8 (torch._int_mm) and fp64 (torch.matmul) GEMM throughput on
+    this GPU, for context beside the roofline denominators."""
+    import torch
+    out = {}
+    n = 8192
+    a = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda")
+    for name, fn, flops in (("int8_int_mm_tops", lambda: torch._int_mm(a, b), 2.0 * n ** 3),):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[name] = flops / (best * 1e-3) / 1e12
+    x = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    y = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(x, y)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    out["fp64_cublas_tflops"] = 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    out["gpu"] = torch.cuda.get_device_name()
+    print(json.dumps(out), flush=True)
+
+
+def run_profile_target(args):
+    """A short, self-contained run for ncu: the c1 plan, one warm-up execute,
+    then --steps executes."""
+    import torch
+    qs = load_engine()
+    A_h, B_h, C_h = host_inputs()
+    sa, sb, sc = shapes()
+    Av = qs.StridedView(torch.from_numpy(A_h).cuda(), sa, colmajor_strides(sa), 0)
+    Bv = qs.StridedView(torch.from_numpy(B_h).cuda(), sb, colmajor_strides(sb), 0)
+    Cv = qs.StridedView(torch.from_numpy(C_h).cuda(), sc, colmajor_strides(sc), 0)
+    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method)
+    qs.execute(plan, ALPHA, BETA)
+    for _ in range(args.steps):
+        qs.execute(plan, ALPHA, BETA)
+    torch.cuda.synchronize()
+    qs.check_status(plan)
+    print(json.dumps({"profile_target": WORKLOAD, "method": plan.method, "steps": args.steps}))
+    plan.release()
 
 
 def cpu_sample(orc, A, B, C, rows, threads):
@@ -194,6 +303,10 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling target: plan, one warm-up execute, --steps executes, exit")
+    ap.add_argument("--peaks", action="store_true",
+                    help="measure cuBLAS int8 (torch._int_mm) and fp64 GEMM throughput, print JSON")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -202,6 +315,12 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.peaks:
+        measure_library_peaks()
+        return
+    if args.profile:
+        run_profile_target(args)
         return
 
     import torch
@@ -248,14 +367,24 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = qs._abi.lib().qs_launch_count()
+    qs.profile(plan, True)  # CUDA events between the plan's launches
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        t_start = time.perf_counter()
         ev0.record(stream)
         for _ in range(args.steps):
             qs.execute(plan, ALPHA, BETA)
         ev1.record(stream)
         torch.cuda.synchronize()
-    launches = qs._abi.lib().qs_launch_count() - launches0
+        launches = qs._abi.lib().qs_launch_count() - launches0
+        # The sampler polls every 100 ms: keep the same load on the GPU (untimed)
+        # until at least 1.5 s of samples exist.
+        while time.perf_counter() - t_start < 1.5:
+            for _ in range(10):
+                qs.execute(plan, ALPHA, BETA)
+            torch.cuda.synchronize()
+    stage_ms, nexec = qs.stage_times(plan)
+    qs.profile(plan, False)
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
         t = torch.tensor([ms], device=dev)
@@ -265,13 +394,7 @@ def main():
     value = world * FLOPS / (ms * 1e-3) / 1e12
 
     # Dominant kernel's own duration: the plan's GEMM stage, timed alone.
-    kern = qs.kernel_profile(plan, ALPHA, BETA, reps=max(3, args.steps // 2)) if hasattr(qs, "kernel_profile") else None
-    peaks, peak_kind = measured_peaks()
-    if kern is not None:
-        roof = kern
-    else:
-        roof = {"bound": "tensor", "achieved": value, "peak": None, "unit": "TFLOP/s", "frac": None,
-                "traffic": None}
+    roof, stages = roofline(plan, stage_ms, nexec)
 
     # End to end through the public API with host buffers.
     A_p = torch.from_numpy(A_h).pin_memory()
@@ -316,7 +439,7 @@ def main():
                        "method": plan.method, "ozaki_slices": plan.ozaki_slices,
                        "l2": "inputs larger than L2 (419 MB), no flush", "parallelism": f"replicas{world}"},
             "rel_err": rel_err, "rel_err_sample": nsamp,
-            "roofline": roof, "peaks_source": peak_kind,
+            "roofline": roof, "stages_ms": stages,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},

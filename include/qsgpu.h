@@ -207,6 +207,21 @@ int qs_contract_noalloc(const qs_view *C, const double *alpha, const qs_view *A,
                         const int64_t *indC, const qs_plan_options *opts,
                         void *stream);
 
+/* Instrumentation.  With profiling enabled, qs_execute records CUDA events
+ * around each of its launches (pack A, pack B, GEMM, fixup for the
+ * tensor-core paths; the single kernel otherwise) for up to 256 executes.
+ * qs_plan_stage_times synchronizes on those events and returns, per stage,
+ * the summed milliseconds, the stage count and the number of executes
+ * recorded; it then clears the record. */
+int qs_plan_profile(qs_plan *plan, int32_t enable);
+int qs_plan_stage_times(qs_plan *plan, double *stage_ms, int32_t max_stages,
+                        int32_t *nstages, int32_t *nexec);
+
+/* Device status word of a plan's tensor-core kernels: synchronizes `stream`,
+ * returns QS_ETIMEOUT (and clears the word) if a bounded wait gave up since
+ * the last check, else QS_OK. */
+int qs_plan_check_status(qs_plan *plan, void *stream);
+
 /* Number of device kernels this library has launched in this process
  * (instrumentation: benchmarks difference it around a timed region). */
 int64_t qs_launch_count(void);

@@ -312,6 +312,26 @@ def execute(plan: ContractPlan, alpha, beta, stream=None) -> torch.Tensor:
     return plan.Cstorage
 
 
+def profile(plan: ContractPlan, enable: bool = True) -> None:
+    """Record CUDA events between the plan's launches on each execute."""
+    _abi.check(_abi.lib().qs_plan_profile(plan._h, int(bool(enable))))
+
+
+def stage_times(plan: ContractPlan):
+    """Summed milliseconds per launch stage since profiling was enabled, and
+    the number of executes recorded (synchronizes on the events)."""
+    ms = (ctypes.c_double * 8)()
+    ns, nx = ctypes.c_int32(), ctypes.c_int32()
+    _abi.check(_abi.lib().qs_plan_stage_times(plan._h, ms, 8, ctypes.byref(ns), ctypes.byref(nx)))
+    return [ms[i] for i in range(ns.value)], nx.value
+
+
+def check_status(plan: ContractPlan, stream=None) -> None:
+    """Raise EngineError if a tensor-core kernel of this plan gave up a
+    bounded wait since the last check (synchronizes the stream)."""
+    _abi.check(_abi.lib().qs_plan_check_status(plan._h, _stream_ptr(stream)))
+
+
 def release(plan: ContractPlan, allocator=None) -> None:
     """``release!``: free the plan's device workspace."""
     plan.release()

@@ -111,6 +111,10 @@ SIGNATURES = {
     "qs_execute_grouped": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P), _DP, _DP, _P]),
     "qs_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
     "qs_launch_count": (ctypes.c_int64, []),
+    "qs_plan_profile": (ctypes.c_int, [_P, ctypes.c_int32]),
+    "qs_plan_stage_times": (ctypes.c_int, [_P, _DP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]),
+    "qs_plan_check_status": (ctypes.c_int, [_P, _P]),
     "qs_contract_noalloc": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
                                            ctypes.POINTER(qs_view), _I64P, _DP, _I64P,
                                            ctypes.POINTER(qs_plan_options), _P]),

@@ -117,6 +117,13 @@ int choose_method(qs_plan *p) {
   return QS_OK;
 }
 
+// The event slot of the next profiled execute (nullptr when profiling is off
+// or the record is full).
+cudaEvent_t *prof_slot(qs_plan *p) {
+  if (!p->prof_on || p->prof_nexec >= qs_plan::kProfExec) return nullptr;
+  return (cudaEvent_t *)p->prof_events.data() + (size_t)p->prof_nexec * (qs_plan::kProfStages + 1);
+}
+
 int scalar_case(int T, const double *v) {
   // Zero/One/general after conversion to the compute type.
   double re = v[0], im = is_complex(T) ? v[1] : 0.0;
@@ -206,13 +213,21 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
   cudaSetDevice(p->device);
   Operands op = make_operands(p);
   cudaError_t e = cudaSuccess;
+  cudaEvent_t *ev = prof_slot(p);
   if (scale_only) {
     if (bcase == 1) return QS_OK;  // C *= 1 is a no-op
+    if (ev) cudaEventRecord(ev[0], st);
     e = launch_scale(p->T, op, beta, bcase, p->c_mfast, st);
     if (e != cudaSuccess) return cuda_fail(e, "scale kernel launch");
+    if (ev) {
+      cudaEventRecord(ev[1], st);
+      p->prof_nstages = 1;
+      ++p->prof_nexec;
+    }
     count_launches(1);
     return QS_OK;
   }
+  if (ev) cudaEventRecord(ev[0], st);
   switch (p->path) {
     case QS_PATH_DOT: e = launch_dot(p->T, op, alpha, beta, bcase, st); break;
     case QS_PATH_OUTER: e = launch_outer(p->T, op, alpha, beta, bcase, p->c_mfast, st); break;
@@ -220,11 +235,73 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
       if (p->method == QS_METHOD_NATIVE) {
         e = launch_direct(p->T, op, alpha, beta, bcase, p->a_mfast, p->b_nfast, st);
       } else {
-        return tc_execute(p, alpha, beta, bcase, st);
+        int rc2 = tc_execute(p, alpha, beta, bcase, st, ev);
+        if (rc2 == QS_OK && ev) ++p->prof_nexec;
+        return rc2;
       }
   }
   if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  if (ev) {
+    cudaEventRecord(ev[1], st);
+    p->prof_nstages = 1;
+    ++p->prof_nexec;
+  }
   count_launches(1);
+  return QS_OK;
+}
+
+int qs_plan_profile(qs_plan *p, int32_t enable) {
+  if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
+  if (p->host_only) return fail(QS_EINVAL, "ArgumentError: a host-only plan cannot be profiled");
+  if (enable && p->prof_events.empty()) {
+    const size_t n = (size_t)qs_plan::kProfExec * (qs_plan::kProfStages + 1);
+    p->prof_events.resize(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+      cudaEvent_t e;
+      cudaError_t rc = cudaEventCreate(&e);
+      if (rc != cudaSuccess) return cuda_fail(rc, "cudaEventCreate");
+      p->prof_events[i] = (void *)e;
+    }
+  }
+  p->prof_on = enable ? 1 : 0;
+  p->prof_nexec = 0;
+  return QS_OK;
+}
+
+int qs_plan_stage_times(qs_plan *p, double *stage_ms, int32_t max_stages, int32_t *nstages,
+                        int32_t *nexec) {
+  if (!p || !stage_ms || !nstages || !nexec) return fail(QS_EINVAL, "ArgumentError: NULL argument");
+  const int ns = p->prof_nstages;
+  for (int s = 0; s < max_stages; ++s) stage_ms[s] = 0.0;
+  for (int x = 0; x < p->prof_nexec; ++x) {
+    cudaEvent_t *ev = (cudaEvent_t *)p->prof_events.data() + (size_t)x * (qs_plan::kProfStages + 1);
+    cudaError_t rc = cudaEventSynchronize(ev[ns]);
+    if (rc != cudaSuccess) return cuda_fail(rc, "cudaEventSynchronize");
+    for (int s = 0; s < ns && s < max_stages; ++s) {
+      float ms = 0.f;
+      rc = cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
+      if (rc != cudaSuccess) return cuda_fail(rc, "cudaEventElapsedTime");
+      stage_ms[s] += ms;
+    }
+  }
+  *nstages = ns;
+  *nexec = p->prof_nexec;
+  p->prof_nexec = 0;
+  return QS_OK;
+}
+
+int qs_plan_check_status(qs_plan *p, void *stream) {
+  if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
+  if (p->host_only || !p->ws.status) return QS_OK;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+  int32_t word = 0;
+  e = cudaMemcpy(&word, p->ws.status, sizeof(word), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (status)");
+  if (word != 0) {
+    cudaMemset(p->ws.status, 0, sizeof(int32_t));
+    return fail(QS_ETIMEOUT, "a bounded device wait gave up (tensor-core kernel aborted)");
+  }
   return QS_OK;
 }
 
@@ -234,6 +311,9 @@ int qs_plan_destroy(qs_plan *p) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaSetDevice(p->device);
+    for (void *e : p->prof_events)
+      if (e) cudaEventDestroy((cudaEvent_t)e);
+    p->prof_events.clear();
     free_workspace(p);
     cudaSetDevice(dev);
   }

@@ -71,6 +71,7 @@ struct Workspace {
   int32_t *expA = nullptr;  // per packed row of A (Ozaki), or nullptr
   int32_t *expB = nullptr;
   int32_t *status = nullptr;  // device status word (bounded waits)
+  void *rowmax = nullptr;     // Ozaki: per-row max |x| bit patterns
   size_t bytes = 0;
   std::vector<void *> owned;  // every cudaMalloc'd pointer, for freeing
 };
@@ -114,6 +115,11 @@ struct qs_plan {
   int c_mfast = 0;  // C's M map is unit-stride
   qs::TensorCoreGeom tc;
   qs::Workspace ws;
+  // Instrumentation (qs_plan_profile): cudaEvent_t handles, kProfStages+1
+  // per recorded execute.
+  static constexpr int kProfExec = 256, kProfStages = 5;
+  int prof_on = 0, prof_nexec = 0, prof_nstages = 0;
+  std::vector<void *> prof_events;
 };
 
 namespace qs {

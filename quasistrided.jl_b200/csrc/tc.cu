@@ -2,8 +2,9 @@
 //
 //  * Float64 as an Ozaki-style split: every row of A and every column of B is
 //    scaled by a power of two (its max-magnitude exponent), cut into s signed
-//    7-bit integer slices, and the slice products are computed exactly on the
-//    integer tensor cores (tcgen05.mma kind::i8, INT32 accumulation in TMEM).
+//    base-254 digits (int8 in [-127, 127]), and the slice products are
+//    computed exactly on the integer tensor cores (tcgen05.mma kind::i8,
+//    INT32 accumulation in TMEM).
 //    Products of equal weight (p + q = t) share one INT32 accumulator; each
 //    diagonal is added into an FP64 running sum kept in TMEM, and the final
 //    alpha/beta epilogue rescales and rounds once to eltype(C).
@@ -59,14 +60,16 @@ __device__ __forceinline__ int64_t panel_tile_base(const PackArgs &a, int64_t ro
   return ((rt * a.kblocks + kb) * a.tile_rows) * kKBytes + sw128_offset((uint32_t)r, (uint32_t)(kbyte & 127));
 }
 
-// 64 rows x 64 K values of X, converted to the compute type, into smem.
-template <class T>
-__device__ __forceinline__ void load_tile64(const PackArgs &a, int64_t r0, int64_t k0, T (*tile)[65]) {
+// A tile of 32 rows x KT K values of X, converted to the compute type, into
+// smem, coalesced along whichever of rows / K is X's unit-stride axis.
+template <class T, int KT>
+__device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t k0, T (*tile)[KT + 1]) {
   const int tid = threadIdx.x;
-#pragma unroll 4
-  for (int i = 0; i < 16; ++i) {
+  constexpr int PER = 32 * KT / 256;
+#pragma unroll 8
+  for (int i = 0; i < PER; ++i) {
     int e = tid + 256 * i, rr, kk;
-    if (a.rfast) { rr = e & 63; kk = e >> 6; } else { kk = e & 63; rr = e >> 6; }
+    if (a.rfast) { rr = e & 31; kk = e >> 5; } else { kk = e % KT; rr = e / KT; }
     int64_t r = r0 + rr, k = k0 + kk;
     T v = (T)0;
     if (r < a.rows && k < a.K) v = Loader<T>::load(a.X, a.Xbase + a.offR[r] + a.offK[k], a.TX, a.conj);
@@ -74,101 +77,101 @@ __device__ __forceinline__ void load_tile64(const PackArgs &a, int64_t r0, int64
   }
 }
 
-// Ozaki slicing of 64 rows: pass 1 finds each row's max magnitude (and any
-// non-finite value), pass 2 writes s digit planes:
-//   x = v * 2^-e (|x| < 1); for p = 1..s: y = 128 x; d_p = trunc(y); x = y - d_p
-// so v = 2^e * (sum_p d_p 2^-7p + r 2^-7s) with |d_p| <= 127, all exact.
-__global__ void __launch_bounds__(256) oz_pack_kernel(PackArgs a) {
-  __shared__ double tile[64][65];
-  const int tid = threadIdx.x;
-  const int row = tid >> 2, part = tid & 3;
-  const int64_t r0 = (int64_t)blockIdx.x * 64;
-  double amax = 0.0;
-  bool bad = false;
-  for (int64_t k0 = 0; k0 < a.K; k0 += 64) {
-    load_tile64<double>(a, r0, k0, tile);
-    __syncthreads();
+// Ozaki pass 1: each row's max magnitude, as the bit pattern of |x| (for
+// non-negative doubles the integer order is the value order, and any NaN or
+// Inf sorts above every finite value).  Grid: 32-row blocks x 128-wide K
+// blocks; one atomicMax per row and block.
+__global__ void __launch_bounds__(256) oz_rowmax_kernel(PackArgs a, unsigned long long *rowmax) {
+  __shared__ double tile[32][129];
+  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 128;
+  load_tile<double, 128>(a, r0, k0, tile);
+  __syncthreads();
+  const int row = threadIdx.x >> 3, part = threadIdx.x & 7;  // 8 threads per row
+  unsigned long long m = 0;
+#pragma unroll
+  for (int kk = 0; kk < 16; ++kk) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(fabs(tile[row][part * 16 + kk]));
+    m = b > m ? b : m;
+  }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
+  }
+  if (part == 0 && r0 + row < a.rows && m) atomicMax(rowmax + r0 + row, m);
+}
+
+// Ozaki pass 2: the digit planes of one 32-row x 128-byte block.  With
+// E = (frexp exponent of the row max) + 1, x = v * 2^-E has |x| < 1/2, and
+//   for p = 1..s: y = 254 x; d_p = rint(y); x = y - d_p
+// gives digits |d_p| <= 127 with v ~= 2^E * sum_p d_p 254^-p; the error is
+// the tail 254^-s plus one rounding of 254 x per digit.  Rows with a NaN or
+// Inf get exponent kNonFinite, zero digits, and are listed for the fixup.
+__global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigned long long *rowmax) {
+  __shared__ double tile[32][129];
+  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 128;
+  load_tile<double, 128>(a, r0, k0, tile);
+  __syncthreads();
+  const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // 16-byte chunk c of the row
+  const int64_t grow = r0 + row;
+  if (grow >= a.rows_pad) return;
+  const unsigned long long mb = grow < a.rows ? rowmax[grow] : 0ull;
+  int E = 0;
+  const bool bad = mb >= 0x7FF0000000000000ull;
+  if (bad) {
+    E = kNonFinite;
+  } else if (mb) {
+    frexp(__longlong_as_double((long long)mb), &E);
+    E += 1;
+  }
+  if (blockIdx.y == 0 && c == 0) {
+    a.exp_out[grow] = E;
+    if (bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
+  }
+  double x[16];
+#pragma unroll
+  for (int kk = 0; kk < 16; ++kk) {
+    const double v = tile[row][c * 16 + kk];
+    x[kk] = (bad || !mb) ? 0.0 : ldexp(v, -E);
+  }
+  const int64_t off = panel_tile_base(a, grow, k0 + c * 16);
+  for (int p = 0; p < a.nslices; ++p) {
+    uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
-      double v = tile[row][part * 16 + kk];
-      if (!isfinite(v)) bad = true;
-      amax = fmax(amax, fabs(v));
+      const double y = x[kk] * 254.0;
+      const double d = rint(y);
+      x[kk] = y - d;
+      const uint32_t byte = (uint32_t)((int32_t)d) & 0xFFu;
+      w[kk >> 2] |= byte << (8 * (kk & 3));
     }
-    __syncthreads();
-  }
-  amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, 1));
-  amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, 2));
-  bad = __shfl_xor_sync(0xffffffffu, (int)bad, 1) || bad;
-  bad = __shfl_xor_sync(0xffffffffu, (int)bad, 2) || bad;
-  int e = 0;
-  if (bad) e = kNonFinite;
-  else if (amax > 0.0) frexp(amax, &e);
-  const int64_t grow = r0 + row;
-  if (part == 0 && grow < a.rows_pad) {
-    a.exp_out[grow] = e;
-    if (bad && grow < a.rows) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
-  }
-  const int64_t kpad = (int64_t)a.kblocks * kKBytes;
-  for (int64_t k0 = 0; k0 < kpad; k0 += 64) {
-    load_tile64<double>(a, r0, k0, tile);
-    __syncthreads();
-    if (grow < a.rows_pad) {
-      double x[16];
-#pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        double v = tile[row][part * 16 + kk];
-        x[kk] = (e == kNonFinite) ? 0.0 : ldexp(v, -e);
-      }
-      const int64_t off = panel_tile_base(a, grow, k0 + part * 16);
-      for (int p = 0; p < a.nslices; ++p) {
-        uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          double y = x[kk] * 128.0;
-          double d = trunc(y);
-          x[kk] = y - d;
-          uint32_t byte = (uint32_t)((int32_t)d) & 0xFFu;
-          w[kk >> 2] |= byte << (8 * (kk & 3));
-        }
-        *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
-      }
-    }
-    __syncthreads();
+    *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
-// Split-BF16 planes: hi = bf16(x), lo = bf16(x - hi), x in FP32.
+// Split-BF16 planes of one 32-row x 64-element block: hi = bf16(x),
+// lo = bf16(x - hi), x in FP32.
 __global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
-  __shared__ float tile[64][65];
-  const int tid = threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.x * 64;
-  const int64_t kpad = (int64_t)a.kblocks * (kKBytes / 2);  // elements
-  for (int64_t k0 = 0; k0 < kpad; k0 += 64) {
-    load_tile64<float>(a, r0, k0, tile);
-    __syncthreads();
+  __shared__ float tile[32][65];
+  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 64;
+  load_tile<float, 64>(a, r0, k0, tile);
+  __syncthreads();
+  const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // 8 values per chunk
+  const int64_t grow = r0 + row;
+  if (grow >= a.rows_pad) return;
+  uint32_t hw[4], lw[4];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int item = tid + 256 * h;  // 64 rows x 8 chunks of 8 values
-      int row = item >> 3, c = item & 7;
-      int64_t grow = r0 + row;
-      if (grow < a.rows_pad) {
-        uint32_t hw[4], lw[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float x0 = tile[row][c * 8 + 2 * q], x1 = tile[row][c * 8 + 2 * q + 1];
-          __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-          __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
-          __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
-          hw[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-          lw[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-        }
-        const int64_t off = panel_tile_base(a, grow, (k0 + c * 8) * 2);
-        *reinterpret_cast<uint4 *>(a.panel + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        *reinterpret_cast<uint4 *>(a.panel + a.plane + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-      }
-    }
-    __syncthreads();
+  for (int q = 0; q < 4; ++q) {
+    const float x0 = tile[row][c * 8 + 2 * q], x1 = tile[row][c * 8 + 2 * q + 1];
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+    const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
+    const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
+    hw[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    lw[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
   }
+  const int64_t off = panel_tile_base(a, grow, (k0 + c * 8) * 2);
+  *reinterpret_cast<uint4 *>(a.panel + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4 *>(a.panel + a.plane + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 
 // ---------------------------------------------------------------- GEMM ---
@@ -191,6 +194,7 @@ struct GemmArgs {
   double alpha, beta;
   int beta_case;
   int *status;
+  double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
 };
 
 template <int KIND>
@@ -379,7 +383,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const uint32_t tacc = tmem + lane_base + buf * BN;
         const uint32_t tsum = tmem + lane_base + 256;
         double w = 1.0;
-        if (KIND == KIND_I8) w = ldexp(1.0, -7 * ((g / a.nkseg) + 2));
+        if (KIND == KIND_I8) w = a.wdiag[g / a.nkseg];
 #pragma unroll 1
         for (int c = 0; c < BN / 16; ++c) {
           uint32_t dr[16], sr[32];
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
               tmem_st16(tsum + 32 * c, sr);
               tmem_st16(tsum + 32 * c + 16, sr + 16);
             } else if (row_store) {
-#pragma unroll 4
+#pragma unroll
               for (int e = 0; e < 16; ++e) {
                 const int jj = 16 * c + e;
                 const int64_t n = n0 + jj;
@@ -425,7 +429,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             }
           } else if (row_ok) {
             const float al = (float)a.alpha, be = (float)a.beta;
-#pragma unroll 4
+#pragma unroll
             for (int e = 0; e < 16; ++e) {
               const int jj = 16 * c + e;
               const int64_t n = n0 + jj;
@@ -517,11 +521,12 @@ int tc_auto_method(const qs_plan *p) {
 }
 
 static int default_slices(int64_t K) {
-  // 7 signed 7-bit slices (28 slice products) reach ~1e-14 relative
-  // Frobenius error at K = 2304 on uniform and 2^+-20-scaled inputs; longer
-  // K gets one more slice per 16x of K (the error grows like sqrt(K)).
-  int s = 7;
-  if (K > 16384) s = 8;
+  // 6 base-254 digits (21 slice products) reach ~1e-14 relative Frobenius
+  // error at K = 2304 on uniform and 2^+-20-scaled inputs (7 signed 7-bit
+  // digits, 28 products, are needed for the same); longer K gets one more
+  // digit (the error grows like sqrt(K)).
+  int s = 6;
+  if (K > 16384) s = 7;
   return s;
 }
 
@@ -587,6 +592,9 @@ int tc_prepare(qs_plan *p) {
     p->ws.expB = b + g.Mp;
     if (cudaMemset(q, 0, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
     p->ws.status = b + n - 1;
+    // row/column max bit patterns, cleared per execute
+    if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
+    p->ws.rowmax = q;
   } else {
     if ((rc = tc_alloc(p, &q, 4 * sizeof(int32_t)))) return rc;
     if (cudaMemset(q, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
@@ -648,7 +656,7 @@ static PackArgs pack_args(const qs_plan *p, int side) {
 }
 
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
-               cudaStream_t st) {
+               cudaStream_t st, cudaEvent_t *ev) {
   const TensorCoreGeom &g = p->tc;
   const bool oz = p->method == QS_METHOD_OZAKI_I8;
   int launches = 0;
@@ -658,12 +666,25 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
+  if (ev) cudaEventRecord(ev[0], st);
+  if (oz) {
+    e = cudaMemsetAsync(p->ws.rowmax, 0, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
+  }
   for (int side = 0; side < 2; ++side) {
     PackArgs pa = pack_args(p, side);
-    dim3 grid((unsigned)cdiv(pa.rows_pad, 64));
-    if (oz) oz_pack_kernel<<<grid, 256, 0, st>>>(pa);
-    else bf16_pack_kernel<<<grid, 256, 0, st>>>(pa);
-    ++launches;
+    if (oz) {
+      unsigned long long *rm = (unsigned long long *)p->ws.rowmax + (side ? g.Mp : 0);
+      dim3 grid((unsigned)cdiv(pa.rows_pad, 32), (unsigned)g.kblocks);
+      oz_rowmax_kernel<<<grid, 256, 0, st>>>(pa, rm);
+      oz_slice_kernel<<<grid, 256, 0, st>>>(pa, rm);
+      launches += 2;
+    } else {
+      dim3 grid((unsigned)cdiv(pa.rows_pad, 32), (unsigned)g.kblocks);
+      bf16_pack_kernel<<<grid, 256, 0, st>>>(pa);
+      ++launches;
+    }
+    if (ev) cudaEventRecord(ev[side + 1], st);
   }
   GemmArgs a;
   a.panelA = (const uint8_t *)p->ws.panelA;
@@ -689,6 +710,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   a.beta = beta[0];
   a.beta_case = beta_case;
   a.status = p->ws.status;
+  for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
   const int tiles = a.mtiles * a.ntiles;
   const int grid = std::min(tiles, num_sms());
   if (oz) {
@@ -697,6 +719,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a);
   }
   ++launches;
+  if (ev) cudaEventRecord(ev[3], st);
   if (oz) {
     Operands op;
     op.A = p->Adata; op.B = p->Bdata; op.C = p->Cdata;
@@ -712,6 +735,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     oz_fixup_kernel<<<64, 256, 0, st>>>(op, alpha[0], beta[0], beta_case, lists, counters,
                                         lists + p->M, counters + 1, p->ws.expA);
     ++launches;
+    if (ev) cudaEventRecord(ev[4], st);
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -720,6 +744,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     return fail(QS_ECUDA, s.str());
   }
   count_launches(launches);
+  p->prof_nstages = oz ? 4 : 3;
   return QS_OK;
 }
 

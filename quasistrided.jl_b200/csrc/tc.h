@@ -14,8 +14,9 @@ void tc_geometry(qs_plan *p);
 // Geometry + device workspace for the packed panels.
 int tc_prepare(qs_plan *p);
 // Pack + tensor-core GEMM + epilogue, enqueued on st.
+// `ev` (nullable) receives an event before the first launch and after each.
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
-               cudaStream_t st);
+               cudaStream_t st, cudaEvent_t *ev = nullptr);
 // Many independent plans as one launch per stage.
 int tc_execute_grouped(int n, qs_plan *const *plans, const double *alpha, const double *beta,
                        cudaStream_t st);
