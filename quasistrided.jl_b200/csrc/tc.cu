@@ -52,7 +52,26 @@ struct PackArgs {
   int nslices;
   int32_t *exp_out;
   int32_t *flag_list, *flag_count;
+  // Complex operands as real matrices (the 1m method): 0 = real; 1 = "1e"
+  // (row 2i = [re, -im], row 2i+1 = [im, re] along K pairs; rows and K are
+  // doubled); 2 = "1r" (K pair = [re; im]; K doubled).  `rows`/`K` above are
+  // the real (virtual) extents; offR/offK index the complex elements.
+  int cmode;
 };
+
+// Element (r, k) of the real (virtual) matrix the panels hold.
+template <class T>
+__device__ __forceinline__ T virtual_elem(const PackArgs &a, int64_t r, int64_t k) {
+  if (a.cmode == 0) return Loader<T>::load(a.X, a.Xbase + a.offR[r] + a.offK[k], a.TX, a.conj);
+  using C = cplx<T>;
+  if (a.cmode == 1) {
+    const C z = Loader<C>::load(a.X, a.Xbase + a.offR[r >> 1] + a.offK[k >> 1], a.TX, a.conj);
+    const int rp = (int)(r & 1), kp = (int)(k & 1);
+    return rp == kp ? z.re : (rp ? z.im : -z.im);
+  }
+  const C z = Loader<C>::load(a.X, a.Xbase + a.offR[r] + a.offK[k >> 1], a.TX, a.conj);
+  return (k & 1) ? z.im : z.re;
+}
 
 __device__ __forceinline__ int64_t panel_tile_base(const PackArgs &a, int64_t row, int64_t kbyte) {
   int64_t rt = row / a.tile_rows, r = row % a.tile_rows;
@@ -72,7 +91,7 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
     if (a.rfast) { rr = e & 31; kk = e >> 5; } else { kk = e % KT; rr = e / KT; }
     int64_t r = r0 + rr, k = k0 + kk;
     T v = (T)0;
-    if (r < a.rows && k < a.K) v = Loader<T>::load(a.X, a.Xbase + a.offR[r] + a.offK[k], a.TX, a.conj);
+    if (r < a.rows && k < a.K) v = virtual_elem<T>(a, r, k);
     tile[rr][kk] = v;
   }
 }
@@ -192,10 +211,55 @@ struct GemmArgs {
   const int64_t *offMC, *offNC;
   int64_t M, N;
   double alpha, beta;
+  double alpha_im, beta_im;
   int beta_case;
+  int cplx;  // 1m: real rows 2i / 2i+1 are Re / Im of complex row i
   int *status;
   double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
 };
+
+// The alpha/beta store of one 16-column chunk of a row of the tile, values
+// in the compute precision R.  Ozaki values are rescaled by 2^(eA + eB) first.
+// Complex (1m): lanes 2l and 2l+1 hold Re and Im of one complex element; the
+// pair is joined with a shuffle and the even lane stores it.
+template <class R>
+__device__ __forceinline__ void store_chunk(const GemmArgs &a, const R (&v)[16], int c, int64_t n0,
+                                            bool row_store, int64_t crow, int lane,
+                                            const int64_t *s_offN, const int32_t *s_expN, int eA) {
+  constexpr int kNF = INT_MIN;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int jj = 16 * c + e;
+    const int64_t n = n0 + jj;
+    const int eB = s_expN[jj];
+    const bool finite = eA != kNF && eB != kNF;
+    R val = v[e];
+    if (sizeof(R) == 8 && finite) val = (R)ldexp((double)val, eA + eB);
+    const bool ok = row_store && n < a.N && finite;
+    const int64_t idx = crow + s_offN[jj];
+    if (a.cplx) {
+      const R other = __shfl_xor_sync(0xffffffffu, val, 1);
+      if (ok && (lane & 1) == 0) {
+        Scalars<cplx<R>> s;
+        s.alpha.re = (R)a.alpha; s.alpha.im = (R)a.alpha_im;
+        s.beta.re = (R)a.beta; s.beta.im = (R)a.beta_im;
+        s.beta_case = a.beta_case;
+        cplx<R> r;
+        r.re = val;
+        r.im = other;
+        const cplx<R> old = a.beta_case == 0 ? tzero<cplx<R>>() : load_c<cplx<R>>(a.C, idx, a.TC);
+        store_c<cplx<R>>(a.C, idx, a.TC, axpby(s, r, old));
+      }
+    } else if (ok) {
+      Scalars<R> s;
+      s.alpha = (R)a.alpha;
+      s.beta = (R)a.beta;
+      s.beta_case = a.beta_case;
+      const R old = a.beta_case == 0 ? (R)0 : load_c<R>(a.C, idx, a.TC);
+      store_c<R>(a.C, idx, a.TC, axpby(s, val, old));
+    }
+  }
+}
 
 template <int KIND>
 struct GemmCfg;
@@ -370,10 +434,10 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         s_expN[j] = (KIND == KIND_I8 && n < a.N) ? a.expB[n] : 0;
       }
       named_bar_sync(1, 128);
-      const int64_t i = m0 + 32 * q + lane;
+      const int64_t i = m0 + 32 * q + lane;  // real (virtual) row
       const bool row_ok = i < a.M;
       const int eA = (KIND == KIND_I8 && row_ok) ? a.expA[i] : 0;
-      const int64_t crow = row_ok ? a.Cbase + a.offMC[i] : 0;
+      const int64_t crow = row_ok ? a.Cbase + a.offMC[a.cplx ? (i >> 1) : i] : 0;
       const bool row_store = row_ok && eA != kNonFinite;
       for (int g = 0; g < nseg; ++g, ++sc) {
         const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
@@ -408,43 +472,14 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
               }
               tmem_st16(tsum + 32 * c, sr);
               tmem_st16(tsum + 32 * c + 16, sr + 16);
-            } else if (row_store) {
-#pragma unroll
-              for (int e = 0; e < 16; ++e) {
-                const int jj = 16 * c + e;
-                const int64_t n = n0 + jj;
-                const int eB = s_expN[jj];
-                if (n < a.N && eB != kNonFinite) {
-                  const double val = ldexp(v[e], eA + eB);
-                  const int64_t idx = crow + s_offN[jj];
-                  double out;
-                  if (a.beta_case == 0) out = a.alpha * val;
-                  else {
-                    const double old = load_c<double>(a.C, idx, a.TC);
-                    out = a.beta_case == 1 ? fma(a.alpha, val, old) : fma(a.alpha, val, a.beta * old);
-                  }
-                  store_c<double>(a.C, idx, a.TC, out);
-                }
-              }
+            } else {
+              store_chunk<double>(a, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
             }
-          } else if (row_ok) {
-            const float al = (float)a.alpha, be = (float)a.beta;
+          } else {
+            float v[16];
 #pragma unroll
-            for (int e = 0; e < 16; ++e) {
-              const int jj = 16 * c + e;
-              const int64_t n = n0 + jj;
-              if (n < a.N) {
-                const float val = __uint_as_float(dr[e]);
-                const int64_t idx = crow + s_offN[jj];
-                float out;
-                if (a.beta_case == 0) out = al * val;
-                else {
-                  const float old = load_c<float>(a.C, idx, a.TC);
-                  out = a.beta_case == 1 ? fmaf(al, val, old) : fmaf(al, val, be * old);
-                }
-                store_c<float>(a.C, idx, a.TC, out);
-              }
-            }
+            for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(dr[e]);
+            store_chunk<float>(a, v, c, n0, row_store, crow, lane, s_offN, s_expN, 0);
           }
         }
         if (KIND == KIND_I8 && !last) tmem_st_wait();
@@ -473,9 +508,13 @@ done:
 // Non-finite rows of A / columns of B (flagged by the pack): those elements
 // of C are computed here directly in FP64 (IEEE semantics), and the GEMM's
 // epilogue skipped them.
-__global__ void oz_fixup_kernel(Operands op, double alpha, double beta, int beta_case,
-                                const int32_t *rows, const int32_t *nrows, const int32_t *cols,
-                                const int32_t *ncols, const int32_t *expA) {
+// T is double or cplx<double>.  The flagged row list holds real (virtual)
+// rows; for the 1m layout rows 2i and 2i+1 are both flagged and the even one
+// stands for complex row i.
+template <class T>
+__global__ void oz_fixup_kernel(Operands op, Scalars<T> s, int cplx, const int32_t *rows,
+                                const int32_t *nrows, const int32_t *cols, const int32_t *ncols,
+                                const int32_t *expA) {
   const int nr = *nrows, nc = *ncols;
   const int64_t total = (int64_t)nr * op.N + (int64_t)nc * op.M;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
@@ -484,26 +523,25 @@ __global__ void oz_fixup_kernel(Operands op, double alpha, double beta, int beta
     if (e < (int64_t)nr * op.N) {
       i = rows[e / op.N];
       j = e % op.N;
+      if (cplx) {
+        if (i & 1) continue;
+        i >>= 1;
+      }
     } else {
       int64_t f = e - (int64_t)nr * op.N;
       j = cols[f / op.M];
       i = f % op.M;
-      if (expA[i] == kNonFinite) continue;  // done by the row pass
+      if (expA[cplx ? 2 * i : i] == kNonFinite) continue;  // done by the row pass
     }
-    double acc = 0.0;
+    T acc = tzero<T>();
     for (int64_t k = 0; k < op.K; ++k) {
-      double x = Loader<double>::load(op.A, op.Abase + op.offMA[i] + op.offKA[k], op.TA, op.conjA);
-      double y = Loader<double>::load(op.B, op.Bbase + op.offNB[j] + op.offKB[k], op.TB, op.conjB);
-      acc = fma(x, y, acc);
+      T x = Loader<T>::load(op.A, op.Abase + op.offMA[i] + op.offKA[k], op.TA, op.conjA);
+      T y = Loader<T>::load(op.B, op.Bbase + op.offNB[j] + op.offKB[k], op.TB, op.conjB);
+      acc = cfma(x, y, acc);
     }
     const int64_t idx = op.Cbase + op.offMC[i] + op.offNC[j];
-    double out;
-    if (beta_case == 0) out = alpha * acc;
-    else {
-      double old = load_c<double>(op.C, idx, op.TC);
-      out = beta_case == 1 ? fma(alpha, acc, old) : fma(alpha, acc, beta * old);
-    }
-    store_c<double>(op.C, idx, op.TC, out);
+    const T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
+    store_c<T>(op.C, idx, op.TC, axpby(s, acc, old));
   }
 }
 
@@ -513,10 +551,10 @@ static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 int tc_auto_method(const qs_plan *p) {
   // The tensor-core paths pay a pack pass and pad to 128-row tiles: worth it
-  // once every extent fills a tile.  Complex plans stay on the gather kernel
-  // until the 1m epilogue lands.
-  if (is_complex(p->T)) return QS_METHOD_NATIVE;
-  if (p->M < 128 || p->N < 128 || p->K < 64) return QS_METHOD_NATIVE;
+  // once every extent fills a tile.  Complex plans run the 1m formulation,
+  // whose real GEMM has 2M rows and 2K columns.
+  const int64_t mr = is_complex(p->T) ? 2 * p->M : p->M;
+  if (mr < 128 || p->N < 128 || p->K < 64) return QS_METHOD_NATIVE;
   return is_double(p->T) ? QS_METHOD_OZAKI_I8 : QS_METHOD_BF16X3;
 }
 
@@ -533,11 +571,18 @@ static int default_slices(int64_t K) {
 void tc_geometry(qs_plan *p) {
   TensorCoreGeom &g = p->tc;
   g = TensorCoreGeom{};
+  // 1m: the real GEMM of a complex plan has 2M rows (A as "1e") and 2K
+  // columns of K (B as "1r").
+  const bool cx = is_complex(p->T);
+  p->complex_mode = cx ? QS_CPLX_1M : QS_CPLX_NONE;
+  g.rows_per_elem_a = cx ? 2 : 1;
+  g.kmul = cx ? 2 : 1;
+  const int64_t Mv = cx ? 2 * p->M : p->M, Kv = cx ? 2 * p->K : p->K;
   if (p->method == QS_METHOD_OZAKI_I8) {
-    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(p->K);
+    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv);
     p->ozaki_slices = g.nslices;
-    g.kblocks = cdiv(p->K, 128);
-    g.mtiles = cdiv(p->M, 128);
+    g.kblocks = cdiv(Kv, 128);
+    g.mtiles = cdiv(Mv, 128);
     g.ntiles = cdiv(p->N, 128);
     g.Mp = g.mtiles * 128;
     g.Np = g.ntiles * 128;
@@ -549,8 +594,8 @@ void tc_geometry(qs_plan *p) {
     g.kseg = (int)std::min<int64_t>(maxkb, g.kblocks);
   } else {
     g.nslices = 2;
-    g.kblocks = cdiv(p->K, 64);
-    g.mtiles = cdiv(p->M, 128);
+    g.kblocks = cdiv(Kv, 64);
+    g.mtiles = cdiv(Mv, 128);
     g.ntiles = cdiv(p->N, 256);
     g.Mp = g.mtiles * 128;
     g.Np = g.ntiles * 256;
@@ -585,7 +630,7 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelB = q;
   if (p->method == QS_METHOD_OZAKI_I8) {
     // exponents (padded rows/cols), non-finite lists, their counters, status
-    size_t n = (size_t)(g.Mp + g.Np + p->M + p->N + 4);
+    size_t n = (size_t)(g.Mp + g.Np + g.Mp + p->N + 4);
     if ((rc = tc_alloc(p, &q, n * sizeof(int32_t)))) return rc;
     int32_t *b = (int32_t *)q;
     p->ws.expA = b;
@@ -628,7 +673,8 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   if (side == 0) {
     a.X = p->Adata; a.Xbase = p->Abase; a.TX = p->TA; a.conj = p->conjA;
     a.offR = p->ws.offM[0]; a.offK = p->ws.offK[0];
-    a.rows = p->M; a.rows_pad = g.Mp; a.tile_rows = 128;
+    a.rows = p->M * g.rows_per_elem_a; a.rows_pad = g.Mp; a.tile_rows = 128;
+    a.cmode = g.kmul == 2 ? 1 : 0;
     a.rfast = p->a_mfast;
     a.panel = (uint8_t *)p->ws.panelA; a.plane = g.plane_bytes_a;
     a.exp_out = p->ws.expA;
@@ -636,17 +682,18 @@ static PackArgs pack_args(const qs_plan *p, int side) {
     a.X = p->Bdata; a.Xbase = p->Bbase; a.TX = p->TB; a.conj = p->conjB;
     a.offR = p->ws.offN[0]; a.offK = p->ws.offK[1];
     a.rows = p->N; a.rows_pad = g.Np; a.tile_rows = p->method == QS_METHOD_BF16X3 ? 256 : 128;
+    a.cmode = g.kmul == 2 ? 2 : 0;
     a.rfast = p->b_nfast;
     a.panel = (uint8_t *)p->ws.panelB; a.plane = g.plane_bytes_b;
     a.exp_out = p->ws.expB;
   }
-  a.K = p->K;
+  a.K = p->K * g.kmul;
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
   if (p->method == QS_METHOD_OZAKI_I8) {
-    int32_t *lists = p->ws.expA + g.Mp + g.Np;
-    int32_t *counters = lists + p->M + p->N;
-    a.flag_list = side == 0 ? lists : lists + p->M;
+    int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: N][2 counters]
+    int32_t *counters = lists + g.Mp + p->N;
+    a.flag_list = side == 0 ? lists : lists + g.Mp;
     a.flag_count = counters + side;
   } else {
     a.flag_list = a.flag_count = nullptr;
@@ -662,7 +709,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   int launches = 0;
   cudaError_t e;
   if (oz) {
-    int32_t *counters = p->ws.expA + g.Mp + g.Np + p->M + p->N;
+    int32_t *counters = p->ws.expA + g.Mp + g.Np + g.Mp + p->N;
     e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
@@ -704,8 +751,11 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   a.TC = p->TC;
   a.offMC = p->ws.offM[1];
   a.offNC = p->ws.offN[1];
-  a.M = p->M;
+  a.M = p->M * g.rows_per_elem_a;
   a.N = p->N;
+  a.cplx = g.kmul == 2;
+  a.alpha_im = alpha[1];
+  a.beta_im = beta[1];
   a.alpha = alpha[0];
   a.beta = beta[0];
   a.beta_case = beta_case;
@@ -731,9 +781,22 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     op.offKA = p->ws.offK[0]; op.offKB = p->ws.offK[1];
     op.M = p->M; op.N = p->N; op.K = p->K;
     int32_t *lists = p->ws.expA + g.Mp + g.Np;
-    int32_t *counters = lists + p->M + p->N;
-    oz_fixup_kernel<<<64, 256, 0, st>>>(op, alpha[0], beta[0], beta_case, lists, counters,
-                                        lists + p->M, counters + 1, p->ws.expA);
+    int32_t *counters = lists + g.Mp + p->N;
+    if (g.kmul == 2) {
+      Scalars<cplx<double>> sc;
+      sc.alpha.re = alpha[0]; sc.alpha.im = alpha[1];
+      sc.beta.re = beta[0]; sc.beta.im = beta[1];
+      sc.beta_case = beta_case;
+      oz_fixup_kernel<cplx<double>><<<64, 256, 0, st>>>(op, sc, 1, lists, counters, lists + g.Mp,
+                                                        counters + 1, p->ws.expA);
+    } else {
+      Scalars<double> sc;
+      sc.alpha = alpha[0];
+      sc.beta = beta[0];
+      sc.beta_case = beta_case;
+      oz_fixup_kernel<double><<<64, 256, 0, st>>>(op, sc, 0, lists, counters, lists + g.Mp,
+                                                  counters + 1, p->ws.expA);
+    }
     ++launches;
     if (ev) cudaEventRecord(ev[4], st);
   }

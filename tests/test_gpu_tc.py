@@ -168,3 +168,88 @@ def test_bf16x3_wide_exponents(qs, orc):
     Bh = orc.HostView(B.host.parent.astype(np.float64), B.host.size, B.host.strides)
     orc.brute(Ch, 1.0, Ah, (1, 2), Bh, (2, 3), 0.0, (1, 3))
     assert rel_fro(got, Ch.parent) <= TOL32
+
+
+def complex_pair(qs, rng, shape, et="ComplexF64"):
+    n = int(np.prod(shape))
+    v = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n))
+    v = v.astype(np.complex128 if et == "ComplexF64" else np.complex64)
+    st, acc = [], 1
+    for s in shape:
+        st.append(acc)
+        acc *= s
+    return Pair(qs, v, tuple(shape), tuple(st))
+
+
+@pytest.mark.parametrize("conj", [(False, False), (True, False), (False, True)])
+@pytest.mark.parametrize("beta", [0.0, 0.5 - 0.25j])
+def test_complex_1m_ozaki(qs, orc, conj, beta):
+    # ComplexF64 through the 1m formulation: A as a 2M x 2K real "1e"
+    # matrix, B as 2K x N "1r", on the INT8 Ozaki kernel.
+    rng = np.random.default_rng(21)
+    M, K, N = 200, 150, 260
+    A = complex_pair(qs, rng, (M, K))
+    B = complex_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "ComplexF64", fill=np.nan if beta == 0 else None)
+    got, ref, plan = run_pair(qs, orc, C, 1.25 + 0.5j, A, (1, 2), B, (2, 3), beta, (1, 3),
+                              conjA=conj[0], conjB=conj[1], precision=1)
+    assert plan.method == "ozaki" and plan.complex_mode == "1m"
+    assert np.all(np.isfinite(got))
+    assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+def test_complex_mps_environment_steps(qs, orc):
+    # The MPS environment update at chi = 64: T1 = L*A, T2 = T1*W,
+    # out = T2*conj(A) (the last step conjugates on load).
+    rng = np.random.default_rng(22)
+    chi, D, d = 64, 5, 2
+    L = complex_pair(qs, rng, (chi, D, chi))
+    A = complex_pair(qs, rng, (chi, d, chi))
+    W = complex_pair(qs, rng, (D, d, D, d))
+    # labels: al=1, w=2, al'=3, s=4, be=5, w'=6, t=7, be'=8
+    T1 = colmajor_pair(qs, rng, (D, chi, d, chi), "ComplexF64", fill=0)
+    got, ref, p1 = run_pair(qs, orc, T1, 1, L, (1, 2, 3), A, (1, 4, 5), 0, (2, 3, 4, 5), precision=1)
+    assert p1.method == "ozaki" and rel_fro(got, ref) <= TOL64
+    T1.host.parent[:] = got  # continue from the device result on both sides
+    T2 = colmajor_pair(qs, rng, (chi, chi, D, d), "ComplexF64", fill=0)
+    got, ref, p2 = run_pair(qs, orc, T2, 1, T1, (2, 3, 4, 5), W, (2, 4, 6, 7), 0, (3, 5, 6, 7), precision=1)
+    assert rel_fro(got, ref) <= TOL64
+    T2.host.parent[:] = got
+    O = colmajor_pair(qs, rng, (chi, D, chi), "ComplexF64", fill=0)
+    got, ref, p3 = run_pair(qs, orc, O, 1, T2, (3, 5, 6, 7), A, (3, 7, 8), 0, (5, 6, 8), conjB=True,
+                            precision=1)
+    assert rel_fro(got, ref) <= TOL64  # N = chi = 64 < one tile: the gather kernel
+
+
+def test_complex_times_real_and_nonfinite(qs, orc):
+    rng = np.random.default_rng(23)
+    M, K, N = 130, 90, 140
+    A = complex_pair(qs, rng, (M, K))
+    b = rng.uniform(-1, 1, K * N)
+    b[5] = np.nan  # column 0 of B
+    B = Pair(qs, b, (K, N), (1, K))
+    C = colmajor_pair(qs, rng, (M, N), "ComplexF64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1)
+    assert plan.method == "ozaki"
+    g = got.reshape(N, M).T
+    r = ref.reshape(N, M).T
+    assert np.array_equal(np.isnan(g), np.isnan(r))
+    fin = np.isfinite(r)
+    assert rel_fro(g[fin], r[fin]) <= TOL64
+
+
+def test_complex_f32_bf16x3(qs, orc):
+    rng = np.random.default_rng(24)
+    M, K, N = 256, 200, 300
+    A = complex_pair(qs, rng, (M, K), "ComplexF32")
+    B = complex_pair(qs, rng, (K, N), "ComplexF32")
+    C = colmajor_pair(qs, rng, (M, N), "ComplexF32")
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3), conjA=True)
+    assert plan.method == "bf16x3" and plan.complex_mode == "1m"
+    qs.execute(plan, 0.5 + 1j, 0.25)
+    got = C.device_parent().astype(np.complex128)
+    Ch = orc.HostView(C.host.parent.astype(np.complex128), C.host.size, C.host.strides)
+    Ah = orc.HostView(A.host.parent.astype(np.complex128), A.host.size, A.host.strides)
+    Bh = orc.HostView(B.host.parent.astype(np.complex128), B.host.size, B.host.strides)
+    orc.brute(Ch, 0.5 + 1j, Ah, (1, 2), Bh, (2, 3), 0.25, (1, 3), conjA=True)
+    assert rel_fro(got, Ch.parent) <= TOL32, rel_fro(got, Ch.parent)
