@@ -240,7 +240,8 @@ def run_profile_target(args):
     Av = qs.StridedView(torch.from_numpy(A_h).cuda(), sa, colmajor_strides(sa), 0)
     Bv = qs.StridedView(torch.from_numpy(B_h).cuda(), sb, colmajor_strides(sb), 0)
     Cv = qs.StridedView(torch.from_numpy(C_h).cuda(), sc, colmajor_strides(sc), 0)
-    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method)
+    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method,
+                            per_product_gemm=args.per_product)
     qs.execute(plan, ALPHA, BETA)
     for _ in range(args.steps):
         qs.execute(plan, ALPHA, BETA)
@@ -300,6 +301,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--method", default="auto", choices=["auto", "native", "ozaki"])
+    ap.add_argument("--per-product", action="store_true",
+                    help="Ozaki: the one-product-per-stage GEMM kernel instead of grouped diagonals")
     ap.add_argument("--cpu-rows", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -341,7 +344,8 @@ def main():
     Av = qs.StridedView(Ad, sa, colmajor_strides(sa), 0)
     Bv = qs.StridedView(Bd, sb, colmajor_strides(sb), 0)
     Cv = qs.StridedView(Cd, sc, colmajor_strides(sc), 0)
-    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method)
+    plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method,
+                            per_product_gemm=args.per_product)
 
     # Accuracy of the measured path: one execution from the seeded C against
     # the FP64 oracle on a sample of C elements (first 2 rows of each 64-block

@@ -93,8 +93,11 @@ enum { QS_CPLX_NONE = 0, QS_CPLX_PLANAR = 1, QS_CPLX_1M = 2 };
 
 /* Plan flags. */
 enum {
-  QS_PLAN_HOST_ONLY = 1 /* plan on the host only: no device workspace; the
-                           plan can be inspected but not executed */
+  QS_PLAN_HOST_ONLY = 1, /* plan on the host only: no device workspace; the
+                            plan can be inspected but not executed */
+  QS_PLAN_PER_PRODUCT_GEMM = 2 /* Ozaki: one slice product per pipeline stage
+                                  (the simpler kernel) instead of grouped
+                                  diagonals with resident slice tiles */
 };
 
 typedef struct qs_view {

@@ -224,7 +224,8 @@ class ContractPlan:
 
 def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=None,
              k_block=None, n_block=None, path_modes: Optional[PathModes] = None,
-             ozaki_slices=0, complex_mode=None, host_only=False) -> _abi.qs_plan_options:
+             ozaki_slices=0, complex_mode=None, host_only=False,
+             per_product_gemm=False) -> _abi.qs_plan_options:
     o = _abi.qs_plan_options()
     o.conjA, o.conjB = int(bool(conjA)), int(bool(conjB))
     o.accumulator = _acc_code(accumulator)
@@ -241,7 +242,7 @@ def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=
     o.unpacked_b_mode = _abi.QS_MODE[pm.unpacked_b]
     o.ozaki_slices = int(ozaki_slices)
     o.complex_mode = _abi.QS_CPLX[complex_mode]
-    o.flags = _abi.QS_PLAN_HOST_ONLY if host_only else 0
+    o.flags = (_abi.QS_PLAN_HOST_ONLY if host_only else 0) | (2 if per_product_gemm else 0)
     return o
 
 
@@ -266,7 +267,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                   kernel=None, conjA=False, conjB=False, m_block=None, k_block=None,
                   n_block=None, allocator=None, accumulator=None,
                   path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
-                  complex_mode=None, host_only=False) -> ContractPlan:
+                  complex_mode=None, host_only=False, per_product_gemm=False) -> ContractPlan:
     """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
 
     Throws ArgumentError / DimensionMismatch on invalid input, before any
@@ -284,7 +285,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
-                 ozaki_slices, complex_mode, host_only)
+                 ozaki_slices, complex_mode, host_only, per_product_gemm)
     h = ctypes.c_void_p()
     _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))

@@ -505,6 +505,296 @@ done:
   }
 }
 
+// ------------------------------------------------------ Ozaki GEMM (v2) ---
+// Slice products grouped so each slice tile is fetched once per K block and
+// group instead of once per product.  Diagonals t = p+q are taken in groups
+// of up to four ({0..3}, {4..7}); every diagonal of a group has its own INT32
+// accumulator (4 x 128 TMEM columns), and the FP64 running sum lives in the
+// registers of eight epilogue warps (64 doubles per thread: one row, one
+// half of the 128 columns).  Per K block a group loads its B slices as a
+// sliding window and streams A_p once; 16 KB tiles move through a ring of
+// kOzSlots shared-memory slots, each freed by the commit after its last MMA.
+
+constexpr int kOzSlots = 13;
+constexpr int kOzMaxLoads = 16, kOzMaxSteps = 40;
+
+struct OzGroup {
+  int t0, t1;  // diagonal range of the group
+  int nloads, nsteps;
+  int8_t load_side[kOzMaxLoads], load_slice[kOzMaxLoads];  // side 0 = A, 1 = B
+  int8_t step_a[kOzMaxSteps], step_b[kOzMaxSteps], step_acc[kOzMaxSteps];
+  uint16_t step_free[kOzMaxSteps];  // loads whose last use is this step
+};
+struct OzSched {
+  int ngroups;
+  OzGroup g[2];
+};
+
+struct GMeta {
+  int nloads, nsteps, t0, t1;
+};
+
+constexpr size_t oz_smem_bytes() {
+  return 1024 + (size_t)kOzSlots * 16384 + 1024 + 128 * (sizeof(int64_t) + sizeof(int32_t)) +
+         1024;  // the schedule, staged from the parameters
+}
+
+// 10 warps: two of the four SM sub-partitions hold three warps, which caps a
+// thread at 168 registers (the launch bound below).
+__global__ void __launch_bounds__(320, 1)
+    oz_gemm_kernel(const __grid_constant__ GemmArgs a, const __grid_constant__ OzSched sch) {
+  constexpr uint32_t TILE = 128 * 128;
+  constexpr uint32_t IDESC = idesc_i8(128, 128);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t *slots = smem;
+  uint64_t *bars = (uint64_t *)(slots + kOzSlots * TILE);
+  uint64_t *full = bars, *empty = bars + kOzSlots, *accf = bars + 2 * kOzSlots, *acce = accf + 4;
+  uint32_t *tmem_slot = (uint32_t *)(acce + 4);
+  volatile int *abort = (volatile int *)(tmem_slot + 1);
+  int64_t *s_offN = (int64_t *)(smem + kOzSlots * TILE + 1024);
+  int32_t *s_expN = (int32_t *)(s_offN + 128);
+  // The schedule in shared memory: one word per product step (load of A in
+  // bits 0-3, load of B in 4-7, accumulator in 8-9, loads freed after the
+  // step in 16-31) and one byte per load (side << 4 | slice).  Read with
+  // dynamic indices in the issue loops, parameters would go through the
+  // slow load path on every step.
+  uint32_t *s_step = (uint32_t *)(s_expN + 128);        // [2][kOzMaxSteps]
+  uint8_t *s_load = (uint8_t *)(s_step + 2 * kOzMaxSteps);  // [2][kOzMaxLoads]
+  GMeta *s_meta = (GMeta *)(s_load + 2 * kOzMaxLoads);      // [2]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kOzSlots; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 4; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 8);
+    }
+    *abort = 0;
+    fence_mbar_init();
+    for (int gi = 0; gi < sch.ngroups; ++gi) {
+      const OzGroup &Gp = sch.g[gi];
+      s_meta[gi] = GMeta{Gp.nloads, Gp.nsteps, Gp.t0, Gp.t1};
+      const OzGroup &G = Gp;
+      for (int st = 0; st < G.nsteps; ++st)
+        s_step[gi * kOzMaxSteps + st] = (uint32_t)(G.step_a[st] & 15) | ((uint32_t)(G.step_b[st] & 15) << 4) |
+                                        ((uint32_t)(G.step_acc[st] & 3) << 8) |
+                                        ((uint32_t)G.step_free[st] << 16);
+      for (int l = 0; l < G.nloads; ++l)
+        s_load[gi * kOzMaxLoads + l] = (uint8_t)((G.load_side[l] << 4) | (G.load_slice[l] & 15));
+    }
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int ntile_total = a.mtiles * a.ntiles;
+
+  if (warp == 0) {
+    // ---------------------------------------------------- producer ----
+    if (lane == 0) {
+      uint32_t L = 0;
+      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+        const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+        for (int gi = 0; gi < sch.ngroups; ++gi) {
+          const GMeta G = s_meta[gi];
+          for (int ks = 0; ks < a.nkseg; ++ks) {
+            const int kb0 = ks * a.kseg_blocks, kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
+            for (int kb = kb0; kb < kb1; ++kb) {
+              for (int l = 0; l < G.nloads; ++l, ++L) {
+                const uint32_t slot = L % kOzSlots, round = L / kOzSlots;
+                if (!mbar_wait(&empty[slot], (round & 1) ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+                mbar_arrive_expect_tx(&full[slot], TILE);
+                const int code = s_load[gi * kOzMaxLoads + l];
+                const uint8_t *src =
+                    (code >> 4) == 0
+                        ? a.panelA + (code & 15) * a.planeA + ((int64_t)mt * a.kblocks + kb) * TILE
+                        : a.panelB + (code & 15) * a.planeB + ((int64_t)nt * a.kblocks + kb) * TILE;
+                bulk_g2s(slots + slot * TILE, src, TILE, &full[slot]);
+              }
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------- MMA ------
+    if (lane == 0) {
+      uint32_t L = 0;
+      uint32_t accpar = 0;  // bit q: parity of accumulator q's use count
+      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+        for (int gi = 0; gi < sch.ngroups; ++gi) {
+          const GMeta G = s_meta[gi];
+          const int nacc = G.t1 - G.t0 + 1;
+          for (int ks = 0; ks < a.nkseg; ++ks) {
+            for (int q = 0; q < nacc; ++q)
+              if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, abort, a.status, QS_ETIMEOUT)) goto done;
+            tc_fence_after();
+            uint32_t started = 0;
+            const int kb0 = ks * a.kseg_blocks, kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
+            for (int kb = kb0; kb < kb1; ++kb) {
+              const uint32_t base = L;
+              uint32_t waited = 0;
+              for (int st = 0; st < G.nsteps; ++st) {
+                const uint32_t word = s_step[gi * kOzMaxSteps + st];
+                const int la = word & 15, lb = (word >> 4) & 15;
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                  const int l = u ? lb : la;
+                  if (!((waited >> l) & 1u)) {
+                    const uint32_t gl = base + l;
+                    if (!mbar_wait(&full[gl % kOzSlots], (gl / kOzSlots) & 1, abort, a.status, QS_ETIMEOUT))
+                      goto done;
+                    waited |= 1u << l;
+                  }
+                }
+                tc_fence_after();
+                const int acc = (word >> 8) & 3;
+                const uint32_t d = tmem + acc * 128;
+                const uint32_t a0 = smem_u32(slots + ((base + la) % kOzSlots) * TILE);
+                const uint32_t b0 = smem_u32(slots + ((base + lb) % kOzSlots) * TILE);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                  const uint32_t accum = (((started >> acc) & 1u) || j > 0) ? 1u : 0u;
+                  mma_i8(d, sw128_kmajor_desc(a0 + 32 * j), sw128_kmajor_desc(b0 + 32 * j), IDESC, accum);
+                }
+                started |= 1u << acc;
+                uint32_t fr = word >> 16;
+                while (fr) {
+                  const int l = __ffs(fr) - 1;
+                  fr &= fr - 1;
+                  tc_commit(&empty[(base + l) % kOzSlots]);
+                }
+              }
+              L += G.nloads;
+            }
+            for (int q = 0; q < nacc; ++q) {
+              tc_commit(&accf[q]);
+              accpar ^= 1u << q;
+            }
+          }
+        }
+      }
+    }
+  } else {
+    // --------------------------------------------------- epilogue -----
+    const int q = warp & 3;               // TMEM lane quarter
+    const int h = (warp - 2) >> 2;        // column half: 0 or 1
+    const int et = threadIdx.x - 64;      // 0..255
+    const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+    uint32_t accpar = 0;  // bit q: parity of accumulator q's use count
+    double sum[64];
+    for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+      const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+      const int64_t m0 = (int64_t)mt * 128, n0 = (int64_t)nt * 128;
+      named_bar_sync(1, 256);
+      if (et < 128) {
+        const int64_t n = n0 + et;
+        s_offN[et] = n < a.N ? a.offNC[n] : 0;
+        s_expN[et] = n < a.N ? a.expB[n] : 0;
+      }
+      named_bar_sync(1, 256);
+      const int64_t i = m0 + 32 * q + lane;
+      const bool row_ok = i < a.M;
+      const int eA = row_ok ? a.expA[i] : 0;
+      const int64_t crow = row_ok ? a.Cbase + a.offMC[a.cplx ? (i >> 1) : i] : 0;
+      const bool row_store = row_ok && eA != kNonFinite;
+      bool first = true;
+      for (int gi = 0; gi < sch.ngroups; ++gi) {
+        const GMeta G = s_meta[gi];
+        const int nacc = G.t1 - G.t0 + 1;
+        for (int ks = 0; ks < a.nkseg; ++ks) {
+          for (int qa = 0; qa < nacc; ++qa) {
+            if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT)) goto done;
+            tc_fence_after();
+            const double w = a.wdiag[G.t0 + qa];
+            const uint32_t taddr = tmem + lane_base + qa * 128 + 64 * h;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              uint32_t dr[16];
+              tmem_ld16(taddr + 16 * c, dr);
+              tmem_ld_wait();
+#pragma unroll
+              for (int e = 0; e < 16; ++e)
+                sum[16 * c + e] = fma((double)(int32_t)dr[e], w, first ? 0.0 : sum[16 * c + e]);
+            }
+            first = false;
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[qa]);
+            accpar ^= 1u << qa;
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = sum[16 * c + e];
+        store_chunk<double>(a, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+      }
+    }
+  }
+done:
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (*abort) {
+    const uint64_t t0 = globaltimer_ns();
+    while (globaltimer_ns() - t0 < 2000000ull) {
+    }
+  }
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// The group schedule of the v2 kernel for s slices (host).
+static OzSched build_oz_sched(int s) {
+  OzSched S;
+  std::memset(&S, 0, sizeof(S));
+  S.ngroups = s > 4 ? 2 : 1;
+  for (int gi = 0; gi < S.ngroups; ++gi) {
+    OzGroup &G = S.g[gi];
+    G.t0 = gi == 0 ? 0 : 4;
+    G.t1 = gi == 0 ? std::min(3, s - 1) : std::min(7, s - 1);
+    int idxA[16], idxB[16];
+    for (int x = 0; x < 16; ++x) idxA[x] = idxB[x] = -1;
+    int last[kOzMaxLoads];
+    for (int p = 0; p <= std::min(G.t1, s - 1); ++p) {
+      const int qlo = std::max(0, G.t0 - p), qhi = std::min(G.t1 - p, s - 1);
+      if (qlo > qhi) continue;
+      for (int q = qhi; q >= qlo; --q)
+        if (idxB[q] < 0) {
+          idxB[q] = G.nloads;
+          G.load_side[G.nloads] = 1;
+          G.load_slice[G.nloads++] = (int8_t)q;
+        }
+      idxA[p] = G.nloads;
+      G.load_side[G.nloads] = 0;
+      G.load_slice[G.nloads++] = (int8_t)p;
+      for (int q = qlo; q <= qhi; ++q) {
+        G.step_a[G.nsteps] = (int8_t)idxA[p];
+        G.step_b[G.nsteps] = (int8_t)idxB[q];
+        G.step_acc[G.nsteps] = (int8_t)(p + q - G.t0);
+        last[idxA[p]] = G.nsteps;
+        last[idxB[q]] = G.nsteps;
+        ++G.nsteps;
+      }
+    }
+    for (int l = 0; l < G.nloads; ++l) G.step_free[last[l]] |= (uint16_t)(1u << l);
+  }
+  return S;
+}
+
 // Non-finite rows of A / columns of B (flagged by the pack): those elements
 // of C are computed here directly in FP64 (IEEE semantics), and the GEMM's
 // epilogue skipped them.
@@ -651,6 +941,8 @@ int tc_prepare(qs_plan *p) {
                          (int)gemm_smem_bytes<KIND_I8>());
     cudaFuncSetAttribute(tc_gemm_kernel<KIND_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)gemm_smem_bytes<KIND_BF16>());
+    cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
     attr_set[0] = attr_set[1] = true;
   }
   return QS_OK;
@@ -764,7 +1056,12 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   const int tiles = a.mtiles * a.ntiles;
   const int grid = std::min(tiles, num_sms());
   if (oz) {
-    tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+    if (g.nslices <= 8 && !(p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM)) {
+      const OzSched sched = build_oz_sched(g.nslices);
+      oz_gemm_kernel<<<grid, 320, oz_smem_bytes(), st>>>(a, sched);
+    } else {
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+    }
   } else {
     tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a);
   }

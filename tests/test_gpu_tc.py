@@ -31,14 +31,16 @@ def uniform_pair(qs, rng, shape, et="Float64", scale_axis=None):
 
 @pytest.mark.parametrize("MKN", [(256, 300, 384), (200, 333, 130), (128, 64, 128), (1000, 129, 777)])
 @pytest.mark.parametrize("beta", [0.0, 1.0, 0.7])
-def test_ozaki_matmul_matches_oracle(qs, orc, MKN, beta):
+@pytest.mark.parametrize("per_product", [False, True])
+def test_ozaki_matmul_matches_oracle(qs, orc, MKN, beta, per_product):
+    # Both GEMM kernels: grouped diagonals (default) and one product per stage.
     M, K, N = MKN
     rng = np.random.default_rng(M * 7 + K)
     A = uniform_pair(qs, rng, (M, K))
     B = uniform_pair(qs, rng, (K, N))
     C = colmajor_pair(qs, rng, (M, N), "Float64", fill=np.nan if beta == 0 else None)
     got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), beta, (1, 3), method="ozaki",
-                              precision=1)
+                              precision=1, per_product_gemm=per_product)
     assert plan.method == "ozaki" and plan.ozaki_slices >= 6
     assert np.all(np.isfinite(got))
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
@@ -97,7 +99,7 @@ def test_ozaki_long_k_segments(qs, orc):
     B = uniform_pair(qs, rng, (K, N))
     C = colmajor_pair(qs, rng, (M, N), "Float64")
     got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), method="ozaki",
-                              ozaki_slices=7, precision=1)
+                              ozaki_slices=8, precision=1)
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
 
 
