@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <sstream>
+#include <utility>
 #include <vector>
 
 #include "kernels.h"
@@ -757,6 +758,73 @@ done:
   }
 }
 
+// ------------------------------------------- Ozaki GEMM, fixed schedule ---
+// The v2 kernel with the schedule a compile-time constant (one instance per
+// slice count): the issue loops unroll into straight-line code, so a product
+// step is its barrier waits (only where a tile is first used), four MMAs and
+// the commits of the tiles it frees.  One thread issues every MMA, so its
+// per-step instruction count bounds the tensor pipe.
+
+template <int S>
+struct OzFixedSched {
+  struct Grp {
+    int t0, t1, nloads, nsteps;
+    int side[kOzMaxLoads], slice[kOzMaxLoads], first_use[kOzMaxLoads];
+    int sa[kOzMaxSteps], sb[kOzMaxSteps], sacc[kOzMaxSteps];
+    unsigned sfree[kOzMaxSteps];
+  };
+  int ngroups;
+  Grp g[2];
+  constexpr OzFixedSched() : ngroups(S > 4 ? 2 : 1), g{} {
+    for (int gi = 0; gi < ngroups; ++gi) {
+      Grp &G = g[gi];
+      G.t0 = gi == 0 ? 0 : 4;
+      G.t1 = gi == 0 ? (S - 1 < 3 ? S - 1 : 3) : (S - 1 < 7 ? S - 1 : 7);
+      int idxA[16] = {}, idxB[16] = {}, last[kOzMaxLoads] = {};
+      for (int x = 0; x < 16; ++x) idxA[x] = idxB[x] = -1;
+      for (int l = 0; l < kOzMaxLoads; ++l) G.first_use[l] = -1;
+      const int pmax = G.t1 < S - 1 ? G.t1 : S - 1;
+      for (int p = 0; p <= pmax; ++p) {
+        const int qlo = G.t0 - p > 0 ? G.t0 - p : 0;
+        const int qhi = G.t1 - p < S - 1 ? G.t1 - p : S - 1;
+        if (qlo > qhi) continue;
+        for (int q = qhi; q >= qlo; --q)
+          if (idxB[q] < 0) {
+            idxB[q] = G.nloads;
+            G.side[G.nloads] = 1;
+            G.slice[G.nloads++] = q;
+          }
+        idxA[p] = G.nloads;
+        G.side[G.nloads] = 0;
+        G.slice[G.nloads++] = p;
+        for (int q = qlo; q <= qhi; ++q) {
+          const int st = G.nsteps++;
+          G.sa[st] = idxA[p];
+          G.sb[st] = idxB[q];
+          G.sacc[st] = p + q - G.t0;
+          if (G.first_use[idxA[p]] < 0) G.first_use[idxA[p]] = st;
+          if (G.first_use[idxB[q]] < 0) G.first_use[idxB[q]] = st;
+          last[idxA[p]] = st;
+          last[idxB[q]] = st;
+        }
+      }
+      for (int l = 0; l < G.nloads; ++l) G.sfree[last[l]] |= 1u << l;
+    }
+  }
+};
+
+// Ring slot and phase parity of load l of a block whose first load has
+// global index L (l < 2 * kOzSlots).
+__device__ __forceinline__ void oz_slot(uint32_t s0, uint32_t par0, int l, uint32_t &slot,
+                                        uint32_t &par) {
+  const uint32_t idx = s0 + (uint32_t)l;
+  const uint32_t w = (idx >= kOzSlots ? 1u : 0u) + (idx >= 2 * kOzSlots ? 1u : 0u);
+  slot = idx - w * kOzSlots;
+  par = par0 ^ (w & 1u);
+}
+
+#include "oz_fixed.cuh"
+
 // The group schedule of the v2 kernel for s slices (host).
 static OzSched build_oz_sched(int s) {
   OzSched S;
@@ -943,6 +1011,10 @@ int tc_prepare(qs_plan *p) {
                          (int)gemm_smem_bytes<KIND_BF16>());
     cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
     attr_set[0] = attr_set[1] = true;
   }
   return QS_OK;
@@ -1056,7 +1128,13 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   const int tiles = a.mtiles * a.ntiles;
   const int grid = std::min(tiles, num_sms());
   if (oz) {
-    if (g.nslices <= 8 && !(p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM)) {
+    if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) {
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+    } else if (g.nslices == 6) {
+      oz_gemm_fixed_kernel<6><<<grid, 320, oz_smem_bytes(), st>>>(a);
+    } else if (g.nslices == 7) {
+      oz_gemm_fixed_kernel<7><<<grid, 320, oz_smem_bytes(), st>>>(a);
+    } else if (g.nslices <= 8) {
       const OzSched sched = build_oz_sched(g.nslices);
       oz_gemm_kernel<<<grid, 320, oz_smem_bytes(), st>>>(a, sched);
     } else {
