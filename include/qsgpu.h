@@ -95,9 +95,12 @@ enum { QS_CPLX_NONE = 0, QS_CPLX_PLANAR = 1, QS_CPLX_1M = 2 };
 enum {
   QS_PLAN_HOST_ONLY = 1, /* plan on the host only: no device workspace; the
                             plan can be inspected but not executed */
-  QS_PLAN_PER_PRODUCT_GEMM = 2 /* Ozaki: one slice product per pipeline stage
-                                  (the simpler kernel) instead of grouped
-                                  diagonals with resident slice tiles */
+  QS_PLAN_PER_PRODUCT_GEMM = 2, /* Ozaki: one slice product per pipeline stage
+                                   (the simpler kernel) instead of grouped
+                                   diagonals with resident slice tiles */
+  QS_PLAN_CUDA_GRAPH = 4 /* qs_execute captures the plan's launches into a
+                            CUDA graph once (again when alpha/beta change)
+                            and replays it on later calls */
 };
 
 typedef struct qs_view {
@@ -186,10 +189,52 @@ int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB,
                           const int64_t *pAB_lin, int64_t *indA,
                           int64_t *indB, int64_t *indC);
 
-/* Grouped execution of many independent plans as one persistent launch over
- * a device problem table (block-sparse contractions).  All plans must be of
- * the same compute type; alpha/beta are per plan ({re, im} pairs, 2*n
- * doubles each). */
+/* Grouped execution of many independent plans: the block-sparse
+ * contraction step of a symmetric tensor network, where each charge sector
+ * is one plan.  No counterpart in the reference, whose engine runs one plan
+ * per contract! call (src/execution/execute.jl:191-210); each plan's result
+ * is that of qs_execute on it.
+ *
+ * Modes:
+ *   QS_GROUP_PERSISTENT  plans sharing a kernel class (compute type for the
+ *                        gather GEMM; method and slice count for the tensor-
+ *                        core paths) run as ONE launch per stage: a grouped
+ *                        pack, a persistent GEMM whose CTAs walk the tiles
+ *                        of a device problem table, one fixup.  Dot, outer
+ *                        and scale plans run as their own launches.
+ *   QS_GROUP_SEQUENTIAL  one qs_execute per plan, in order (the baseline).
+ *   QS_GROUP_GRAPH       (flag) the launches of an execute are captured into
+ *                        a CUDA graph once and replayed; alpha/beta changes
+ *                        re-capture.
+ * The plans must not share C with each other, must not be executed on their
+ * own while the group is in use, and stay owned by the caller (destroy the
+ * group first).  All bounds are checked for every plan before any launch. */
+typedef struct qs_group qs_group;
+enum {
+  QS_GROUP_PERSISTENT = 0,
+  QS_GROUP_SEQUENTIAL = 1,
+  QS_GROUP_GRAPH = 2
+};
+
+typedef struct qs_group_info {
+  int32_t nplans;
+  int32_t launches;      /* kernels per execute (last execute) */
+  int32_t native_plans;  /* plans in grouped gather-GEMM launches */
+  int32_t tc_plans;      /* plans in grouped tensor-core launches */
+  int32_t single_plans;  /* plans run as their own launches */
+  int32_t classes;       /* grouped launch classes in use */
+  int64_t tiles;         /* tensor-core tiles per execute */
+  int64_t table_bytes;   /* device bytes of the problem tables */
+} qs_group_info;
+
+int qs_group_create(int32_t n, qs_plan *const *plans, int32_t mode, qs_group **out);
+/* alpha/beta: {re, im} per plan (2*n doubles each).  Enqueued on `stream`. */
+int qs_group_execute(qs_group *g, const double *alpha, const double *beta, void *stream);
+int qs_group_get_info(const qs_group *g, qs_group_info *info);
+int qs_group_destroy(qs_group *g);
+
+/* One-shot grouped execute: create (QS_GROUP_PERSISTENT), execute, wait for
+ * the stream, destroy. */
 int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha,
                        const double *beta, void *stream);
 

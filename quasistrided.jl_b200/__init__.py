@@ -37,7 +37,7 @@ __all__ = [
     "StridedView", "plan_contract", "execute", "contract", "ContractPlan", "PathModes",
     "QuasiStridedBackend", "tensorcontract", "contraction_labels", "release",
     "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "colmajor",
-    "execute_grouped",
+    "execute_grouped", "ContractGroup",
 ]
 
 _DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
@@ -225,7 +225,7 @@ class ContractPlan:
 def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=None,
              k_block=None, n_block=None, path_modes: Optional[PathModes] = None,
              ozaki_slices=0, complex_mode=None, host_only=False,
-             per_product_gemm=False) -> _abi.qs_plan_options:
+             per_product_gemm=False, cuda_graph=False) -> _abi.qs_plan_options:
     o = _abi.qs_plan_options()
     o.conjA, o.conjB = int(bool(conjA)), int(bool(conjB))
     o.accumulator = _acc_code(accumulator)
@@ -242,7 +242,8 @@ def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=
     o.unpacked_b_mode = _abi.QS_MODE[pm.unpacked_b]
     o.ozaki_slices = int(ozaki_slices)
     o.complex_mode = _abi.QS_CPLX[complex_mode]
-    o.flags = (_abi.QS_PLAN_HOST_ONLY if host_only else 0) | (2 if per_product_gemm else 0)
+    o.flags = ((_abi.QS_PLAN_HOST_ONLY if host_only else 0) | (2 if per_product_gemm else 0) |
+               (4 if cuda_graph else 0))
     return o
 
 
@@ -267,11 +268,14 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                   kernel=None, conjA=False, conjB=False, m_block=None, k_block=None,
                   n_block=None, allocator=None, accumulator=None,
                   path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
-                  complex_mode=None, host_only=False, per_product_gemm=False) -> ContractPlan:
+                  complex_mode=None, host_only=False, per_product_gemm=False,
+                  cuda_graph=False) -> ContractPlan:
     """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
 
     Throws ArgumentError / DimensionMismatch on invalid input, before any
     device work.  ``kernel`` names a method ("native", "ozaki", "bf16x3");
+    ``cuda_graph`` makes ``execute`` replay a captured CUDA graph of the
+    plan's launches (re-captured when alpha/beta change);
     ``allocator`` is accepted for signature parity (the plan allocates its
     workspace in device memory).  ``host_only`` plans without touching the
     device (inspection only).
@@ -285,7 +289,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
-                 ozaki_slices, complex_mode, host_only, per_product_gemm)
+                 ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph)
     h = ctypes.c_void_p()
     _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))
@@ -354,17 +358,66 @@ def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, 
     return C
 
 
+def _scalar_pairs(values, n):
+    arr = (ctypes.c_double * (2 * max(1, n)))()
+    for i in range(n):
+        z = complex(values[i])
+        arr[2 * i], arr[2 * i + 1] = z.real, z.imag
+    return arr
+
+
+class ContractGroup:
+    """Many independent plans executed together (qs_group_*).
+
+    mode: "persistent" (one launch per stage and kernel class, over a device
+    problem table), "sequential" (one execute per plan) — either with
+    graph=True to capture the launches into a CUDA graph replayed on later
+    executes.  The plans stay owned by the caller and must outlive the group.
+    """
+
+    def __init__(self, plans: Sequence[ContractPlan], mode: str = "persistent", graph: bool = False):
+        modes = {"persistent": _abi.QS_GROUP_PERSISTENT, "sequential": _abi.QS_GROUP_SEQUENTIAL}
+        if mode not in modes:
+            raise ArgumentError(f"unknown group mode {mode!r}")
+        self.plans = list(plans)
+        n = len(self.plans)
+        arr = (ctypes.c_void_p * max(1, n))(*[p._h for p in self.plans])
+        h = ctypes.c_void_p()
+        flag = modes[mode] | (_abi.QS_GROUP_GRAPH if graph else 0)
+        _abi.check(_abi.lib().qs_group_create(n, arr, flag, ctypes.byref(h)))
+        self._h = h
+        self.mode, self.graph = mode, graph
+
+    def execute(self, alphas, betas, stream=None) -> None:
+        n = len(self.plans)
+        if len(alphas) != n or len(betas) != n:
+            raise ArgumentError("one alpha and one beta per plan")
+        _abi.check(_abi.lib().qs_group_execute(self._h, _scalar_pairs(alphas, n), _scalar_pairs(betas, n),
+                                               _stream_ptr(stream)))
+
+    def info(self) -> dict:
+        inf = _abi.qs_group_info()
+        _abi.check(_abi.lib().qs_group_get_info(self._h, ctypes.byref(inf)))
+        return {k: getattr(inf, k) for k, _ in _abi.qs_group_info._fields_}
+
+    def release(self) -> None:
+        if getattr(self, "_h", None):
+            _abi.lib().qs_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
 def execute_grouped(plans: Sequence[ContractPlan], alphas, betas, stream=None) -> None:
-    """Execute many independent plans as grouped launches (block-sparse steps)."""
+    """One-shot grouped execute (persistent mode); waits for the stream."""
     n = len(plans)
     arr = (ctypes.c_void_p * max(1, n))(*[p._h for p in plans])
-    al = (ctypes.c_double * (2 * max(1, n)))()
-    be = (ctypes.c_double * (2 * max(1, n)))()
-    for i in range(n):
-        za, zb = complex(alphas[i]), complex(betas[i])
-        al[2 * i], al[2 * i + 1] = za.real, za.imag
-        be[2 * i], be[2 * i + 1] = zb.real, zb.imag
-    _abi.check(_abi.lib().qs_execute_grouped(n, arr, al, be, _stream_ptr(stream)))
+    _abi.check(_abi.lib().qs_execute_grouped(n, arr, _scalar_pairs(alphas, n), _scalar_pairs(betas, n),
+                                             _stream_ptr(stream)))
 
 
 # ------------------------------------------------------- TensorOperations ---

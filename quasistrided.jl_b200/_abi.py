@@ -93,6 +93,23 @@ class qs_plan_info(ctypes.Structure):
     ]
 
 
+class qs_group_info(ctypes.Structure):
+    _fields_ = [
+        ("nplans", ctypes.c_int32),
+        ("launches", ctypes.c_int32),
+        ("native_plans", ctypes.c_int32),
+        ("tc_plans", ctypes.c_int32),
+        ("single_plans", ctypes.c_int32),
+        ("classes", ctypes.c_int32),
+        ("tiles", ctypes.c_int64),
+        ("table_bytes", ctypes.c_int64),
+    ]
+
+
+QS_GROUP_PERSISTENT = 0
+QS_GROUP_SEQUENTIAL = 1
+QS_GROUP_GRAPH = 2
+
 # Every symbol the header declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I64P = ctypes.POINTER(ctypes.c_int64)
@@ -109,6 +126,10 @@ SIGNATURES = {
     "qs_contraction_labels": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _I64P, _I64P, _I64P,
                                              _I64P, _I64P, _I64P]),
     "qs_execute_grouped": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P), _DP, _DP, _P]),
+    "qs_group_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P), ctypes.c_int32, ctypes.POINTER(_P)]),
+    "qs_group_execute": (ctypes.c_int, [_P, _DP, _DP, _P]),
+    "qs_group_get_info": (ctypes.c_int, [_P, ctypes.POINTER(qs_group_info)]),
+    "qs_group_destroy": (ctypes.c_int, [_P]),
     "qs_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
     "qs_launch_count": (ctypes.c_int64, []),
     "qs_plan_profile": (ctypes.c_int, [_P, ctypes.c_int32]),

@@ -29,6 +29,45 @@ static std::atomic<int64_t> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 }  // namespace qs
 
+namespace qs {
+Operands make_operands(const qs_plan *p) {
+  Operands op;
+  op.A = p->Adata;
+  op.B = p->Bdata;
+  op.C = p->Cdata;
+  op.Abase = p->Abase;
+  op.Bbase = p->Bbase;
+  op.Cbase = p->Cbase;
+  op.TA = p->TA;
+  op.TB = p->TB;
+  op.TC = p->TC;
+  op.conjA = p->conjA;
+  op.conjB = p->conjB;
+  op.offMA = p->ws.offM[0];
+  op.offMC = p->ws.offM[1];
+  op.offNB = p->ws.offN[0];
+  op.offNC = p->ws.offN[1];
+  op.offKA = p->ws.offK[0];
+  op.offKB = p->ws.offK[1];
+  op.M = p->M;
+  op.N = p->N;
+  op.K = p->K;
+  return op;
+}
+
+int scalar_case(int T, const double *v) {
+  // Zero/One/general after conversion to the compute type.
+  double re = v[0], im = is_complex(T) ? v[1] : 0.0;
+  if (!is_double(T)) {
+    re = (double)(float)re;
+    im = (double)(float)im;
+  }
+  if (re == 0.0 && im == 0.0) return 0;
+  if (re == 1.0 && im == 0.0) return 1;
+  return 2;
+}
+}  // namespace qs
+
 namespace {
 
 int cuda_fail(cudaError_t e, const char *what) {
@@ -76,31 +115,6 @@ int upload_offsets(qs_plan *p, const Group &g, int64_t **dst) {
   return QS_OK;
 }
 
-Operands make_operands(const qs_plan *p) {
-  Operands op;
-  op.A = p->Adata;
-  op.B = p->Bdata;
-  op.C = p->Cdata;
-  op.Abase = p->Abase;
-  op.Bbase = p->Bbase;
-  op.Cbase = p->Cbase;
-  op.TA = p->TA;
-  op.TB = p->TB;
-  op.TC = p->TC;
-  op.conjA = p->conjA;
-  op.conjB = p->conjB;
-  op.offMA = p->ws.offM[0];
-  op.offMC = p->ws.offM[1];
-  op.offNB = p->ws.offN[0];
-  op.offNC = p->ws.offN[1];
-  op.offKA = p->ws.offK[0];
-  op.offKB = p->ws.offK[1];
-  op.M = p->M;
-  op.N = p->N;
-  op.K = p->K;
-  return op;
-}
-
 // Method for the nest path: the requested one if valid, else the
 // autotuner's choice (tensor-core paths once the problem fills a tile).
 int choose_method(qs_plan *p) {
@@ -124,16 +138,68 @@ cudaEvent_t *prof_slot(qs_plan *p) {
   return (cudaEvent_t *)p->prof_events.data() + (size_t)p->prof_nexec * (qs_plan::kProfStages + 1);
 }
 
-int scalar_case(int T, const double *v) {
-  // Zero/One/general after conversion to the compute type.
-  double re = v[0], im = is_complex(T) ? v[1] : 0.0;
-  if (!is_double(T)) {
-    re = (double)(float)re;
-    im = (double)(float)im;
+void destroy_graph(qs_plan *p) {
+  if (p->graph_exec) cudaGraphExecDestroy((cudaGraphExec_t)p->graph_exec);
+  if (p->graph) cudaGraphDestroy((cudaGraph_t)p->graph);
+  p->graph_exec = nullptr;
+  p->graph = nullptr;
+}
+
+}  // namespace
+
+extern "C" int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream);
+
+namespace {
+
+// execute! on a reused plan as a CUDA graph: the launches of one execute are
+// captured on a private stream (capture of the legacy default stream is not
+// allowed) and the instantiated graph is replayed on the caller's stream.
+// alpha/beta are baked into the captured kernel parameters, so a change of
+// either re-captures.
+int execute_graph(qs_plan *p, const double *alpha, const double *beta, cudaStream_t st) {
+  const bool same = p->graph_exec && p->gal[0] == alpha[0] && p->gal[1] == alpha[1] &&
+                    p->gbe[0] == beta[0] && p->gbe[1] == beta[1];
+  cudaError_t e;
+  if (!same) {
+    destroy_graph(p);
+    if (!p->cap_stream) {
+      cudaStream_t cs;
+      e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreateWithFlags");
+      p->cap_stream = (void *)cs;
+    }
+    cudaStream_t cs = (cudaStream_t)p->cap_stream;
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+    p->capturing = 1;
+    const int prof = p->prof_on;
+    p->prof_on = 0;  // no event records inside the graph
+    int rc = qs_execute(p, alpha, beta, (void *)cs);
+    p->prof_on = prof;
+    p->capturing = 0;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(cs, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    cudaGraphExec_t x;
+    e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    p->graph = (void *)g;
+    p->graph_exec = (void *)x;
+    p->gal[0] = alpha[0];
+    p->gal[1] = alpha[1];
+    p->gbe[0] = beta[0];
+    p->gbe[1] = beta[1];
   }
-  if (re == 0.0 && im == 0.0) return 0;
-  if (re == 1.0 && im == 0.0) return 1;
-  return 2;
+  e = cudaGraphLaunch((cudaGraphExec_t)p->graph_exec, st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+  return QS_OK;
 }
 
 }  // namespace
@@ -204,6 +270,7 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
     // NaN alpha is a legal value: it propagates like the reference.
   }
   cudaStream_t st = (cudaStream_t)stream;
+  if ((p->opts.flags & QS_PLAN_CUDA_GRAPH) && !p->capturing) return execute_graph(p, alpha, beta, st);
   int acase = scalar_case(p->T, alpha);
   int bcase = scalar_case(p->T, beta);
   if (p->path == QS_PATH_EMPTY) return QS_OK;
@@ -314,6 +381,9 @@ int qs_plan_destroy(qs_plan *p) {
     for (void *e : p->prof_events)
       if (e) cudaEventDestroy((cudaEvent_t)e);
     p->prof_events.clear();
+    destroy_graph(p);
+    if (p->cap_stream) cudaStreamDestroy((cudaStream_t)p->cap_stream);
+    p->cap_stream = nullptr;
     free_workspace(p);
     cudaSetDevice(dev);
   }
@@ -403,13 +473,6 @@ int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB, const int64_t *p
   }
   for (int i = 0; i < NoA + NoB; ++i) indC[i] = pAB_lin[i];
   return QS_OK;
-}
-
-int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha, const double *beta,
-                       void *stream) {
-  if (n < 0 || (n > 0 && (!plans || !alpha || !beta)))
-    return fail(QS_EINVAL, "ArgumentError: invalid grouped arguments");
-  return tc_execute_grouped(n, plans, alpha, beta, (cudaStream_t)stream);
 }
 
 size_t qs_last_error(char *buf, size_t n);

@@ -11,6 +11,10 @@
 //   outer         <- execute_path!(OuterPath) (src/execution/outer.jl:10-69)
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -53,16 +57,17 @@ struct DirectCfg {
   static constexpr int B_PER_THREAD = BN * BK / kThreads;
 };
 
+// The tile (bx, by) of one problem; the whole CTA calls it.
 template <class T, int BM, int BN, int BK>
-__global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T> s, int a_mfast,
-                                                          int b_nfast) {
+__device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scalars<T> &s,
+                                                 int a_mfast, int b_nfast, int64_t bx, int64_t by) {
   using Cfg = DirectCfg<T, BM, BN, BK>;
   constexpr int TM = Cfg::TM, TN = Cfg::TN;
   __shared__ T As[2][BK][BM];
   __shared__ T Bs[2][BK][BN];
   const int tid = threadIdx.x;
   const int tx = tid % 16, ty = tid / 16;
-  const int64_t m0 = (int64_t)blockIdx.x * BM, n0 = (int64_t)blockIdx.y * BN;
+  const int64_t m0 = bx * BM, n0 = by * BN;
 
   T acc[TM][TN];
 #pragma unroll
@@ -152,6 +157,40 @@ __global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T
       store_c<T>(op.C, idx, op.TC, axpby(s, acc[i][j], old));
     }
   }
+}
+
+template <class T, int BM, int BN, int BK>
+__global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T> s, int a_mfast,
+                                                          int b_nfast) {
+  direct_gemm_tile<T, BM, BN, BK>(op, s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+}
+
+// Grouped: CTA b runs tile b - block_start of the problem whose block range
+// holds b (binary search over the table); problems sorted by K descending
+// so that the longest tiles start first.
+template <class T>
+struct NativeJob {
+  Operands op;
+  Scalars<T> s;
+  int a_mfast, b_nfast;
+  int gx;  // tiles along M
+  int block_start;
+};
+
+template <class T, int BM, int BN, int BK>
+__global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJob<T> *jobs, int njobs) {
+  int lo = 0, hi = njobs - 1;
+  const int b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].block_start <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const NativeJob<T> &j = jobs[lo];
+  const int lb = b - j.block_start;
+  const Operands op = j.op;
+  const Scalars<T> s = j.s;
+  direct_gemm_tile<T, BM, BN, BK>(op, s, j.a_mfast, j.b_nfast, lb % j.gx, lb / j.gx);
 }
 
 // ---------------------------------------------------------------- dot ----
@@ -377,6 +416,65 @@ cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const d
     case QS_F64: return launch_outer_t<double>(op, alpha, beta, beta_case, mfast, st);
     case QS_C32: return launch_outer_t<cplx<float>>(op, alpha, beta, beta_case, mfast, st);
     default: return launch_outer_t<cplx<double>>(op, alpha, beta, beta_case, mfast, st);
+  }
+}
+
+// Tile shape per compute type (BM, BN, BK).
+template <class T> struct DirectShape { static constexpr int BM = 64, BN = 64, BK = 16; };
+template <> struct DirectShape<cplx<float>> { static constexpr int BM = 32, BN = 32, BK = 16; };
+template <> struct DirectShape<cplx<double>> { static constexpr int BM = 32, BN = 32, BK = 16; };
+
+template <class T>
+static int native_group_build_t(NativeGroup &g, const Operands *ops, const double *alpha,
+                                const double *beta, const int *bcase) {
+  using Sh = DirectShape<T>;
+  const int n = (int)g.plans.size();
+  std::vector<NativeJob<T>> jobs(n);
+  int64_t blocks = 0;
+  for (int i = 0; i < n; ++i) {
+    const int k = g.idx[i];
+    NativeJob<T> &j = jobs[i];
+    j.op = ops[i];
+    j.s = make_scalars<T>(alpha + 2 * k, beta + 2 * k, bcase[k]);
+    j.a_mfast = g.plans[i]->a_mfast;
+    j.b_nfast = g.plans[i]->b_nfast;
+    const int64_t gx = (j.op.M + Sh::BM - 1) / Sh::BM, gy = (j.op.N + Sh::BN - 1) / Sh::BN;
+    if (gx > INT32_MAX || blocks + gx * gy > INT32_MAX) return fail(QS_EINVAL, "ArgumentError: grouped launch too large");
+    j.gx = (int)gx;
+    j.block_start = (int)blocks;
+    blocks += gx * gy;
+  }
+  g.blocks = (int)blocks;
+  g.image.resize(n * sizeof(NativeJob<T>));
+  std::memcpy(g.image.data(), jobs.data(), g.image.size());
+  return QS_OK;
+}
+
+int native_group_build(NativeGroup &g, const Operands *ops, const double *alpha, const double *beta,
+                       const int *bcase) {
+  switch (g.T) {
+    case QS_F32: return native_group_build_t<float>(g, ops, alpha, beta, bcase);
+    case QS_F64: return native_group_build_t<double>(g, ops, alpha, beta, bcase);
+    case QS_C32: return native_group_build_t<cplx<float>>(g, ops, alpha, beta, bcase);
+    default: return native_group_build_t<cplx<double>>(g, ops, alpha, beta, bcase);
+  }
+}
+
+template <class T>
+static cudaError_t native_group_launch_t(const NativeGroup &g, cudaStream_t st) {
+  using Sh = DirectShape<T>;
+  direct_gemm_grouped_kernel<T, Sh::BM, Sh::BN, Sh::BK>
+      <<<g.blocks, 256, 0, st>>>((const NativeJob<T> *)g.dev, (int)g.plans.size());
+  return cudaGetLastError();
+}
+
+cudaError_t native_group_launch(const NativeGroup &g, cudaStream_t st) {
+  if (g.plans.empty()) return cudaSuccess;
+  switch (g.T) {
+    case QS_F32: return native_group_launch_t<float>(g, st);
+    case QS_F64: return native_group_launch_t<double>(g, st);
+    case QS_C32: return native_group_launch_t<cplx<float>>(g, st);
+    default: return native_group_launch_t<cplx<double>>(g, st);
   }
 }
 

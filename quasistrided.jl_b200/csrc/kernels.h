@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "device_common.cuh"
 #include "qs_internal.h"
 
@@ -19,5 +22,26 @@ cudaError_t launch_dot(int T, const Operands &op, const double *alpha, const dou
                        int beta_case, cudaStream_t st);
 cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const double *beta,
                          int beta_case, int mfast, cudaStream_t st);
+
+// Native (gather) GEMMs of many plans of one compute type as one launch.
+struct NativeGroup {
+  int T = 0;
+  std::vector<qs_plan *> plans;  // K-descending
+  std::vector<int> idx;          // position of each plan in the group's alpha/beta arrays
+  std::vector<uint8_t> image;    // host image of the job table
+  void *dev = nullptr;
+  size_t dev_bytes = 0;
+  int blocks = 0;
+};
+// ops[i] are the operands of plans[i]; alpha/beta hold 2 doubles per plan of
+// the group, bcase one int per plan.
+int native_group_build(NativeGroup &g, const Operands *ops, const double *alpha, const double *beta,
+                       const int *bcase);
+cudaError_t native_group_launch(const NativeGroup &g, cudaStream_t st);
+
+// The operands of a plan as the kernels read them.
+Operands make_operands(const qs_plan *p);
+// Zero (0), One (1) or general (2) after conversion to compute type T.
+int scalar_case(int T, const double *v);
 
 }  // namespace qs

@@ -164,8 +164,11 @@ __device__ __forceinline__ bool oz_drain_group(const GemmArgs &a, uint32_t &accp
   return true;
 }
 
-template <int S>
-__global__ void __launch_bounds__(320, 1) oz_gemm_fixed_kernel(const __grid_constant__ GemmArgs a) {
+// GROUPED: tiles come from the problem table gt (a grouped launch); else the
+// launch is one problem, a, and gt is unused.
+template <int S, bool GROUPED>
+__global__ void __launch_bounds__(320, 1)
+    oz_gemm_fixed_kernel(const __grid_constant__ GemmArgs a, const GemmTable gt) {
   constexpr uint32_t TILE = 128 * 128;
   constexpr int NG = kOzSched<S>.ngroups;
   extern __shared__ uint8_t smem_raw[];
@@ -177,6 +180,8 @@ __global__ void __launch_bounds__(320, 1) oz_gemm_fixed_kernel(const __grid_cons
   volatile int *abort = (volatile int *)(tmem_slot + 1);
   int64_t *s_offN = (int64_t *)(smem + kOzSlots * TILE + 1024);
   int32_t *s_expN = (int32_t *)(s_offN + 128);
+  GemmArgs *s_args = reinterpret_cast<GemmArgs *>(s_expN + 128);
+  static_assert(sizeof(GemmArgs) % 4 == 0 && sizeof(GemmArgs) <= 1024, "staged GemmArgs");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -199,26 +204,28 @@ __global__ void __launch_bounds__(320, 1) oz_gemm_fixed_kernel(const __grid_cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int ntile_total = a.mtiles * a.ntiles;
+  const int ntile_total = GROUPED ? gt.tile_start[gt.nprob] : a.mtiles * a.ntiles;
 
   if (warp == 0) {
     if (lane == 0) {
       uint32_t L = 0;
       OzLoadCtx c;
       c.slots = slots;
-      c.planeA = a.planeA;
-      c.planeB = a.planeB;
       c.full = full;
       c.empty = empty;
       c.abort = abort;
       c.status = a.status;
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
-        const int mt = tile / a.ntiles, nt = tile % a.ntiles;
-        const uint8_t *tileA = a.panelA + (int64_t)mt * a.kblocks * TILE;
-        const uint8_t *tileB = a.panelB + (int64_t)nt * a.kblocks * TILE;
-        if (!oz_produce_group<S, 0>(a, L, c, tileA, tileB)) break;
+        int lt;
+        const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
+        const int mt = lt / P.ntiles, nt = lt % P.ntiles;
+        c.planeA = P.planeA;
+        c.planeB = P.planeB;
+        const uint8_t *tileA = P.panelA + (int64_t)mt * P.kblocks * TILE;
+        const uint8_t *tileB = P.panelB + (int64_t)nt * P.kblocks * TILE;
+        if (!oz_produce_group<S, 0>(P, L, c, tileA, tileB)) break;
         if constexpr (NG > 1)
-          if (!oz_produce_group<S, 1>(a, L, c, tileA, tileB)) break;
+          if (!oz_produce_group<S, 1>(P, L, c, tileA, tileB)) break;
       }
     }
   } else if (warp == 1) {
@@ -232,9 +239,11 @@ __global__ void __launch_bounds__(320, 1) oz_gemm_fixed_kernel(const __grid_cons
       c.abort = abort;
       c.status = a.status;
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
-        if (!oz_mma_group<S, 0>(a, L, accpar, c, acce, accf)) break;
+        int lt;
+        const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
+        if (!oz_mma_group<S, 0>(P, L, accpar, c, acce, accf)) break;
         if constexpr (NG > 1)
-          if (!oz_mma_group<S, 1>(a, L, accpar, c, acce, accf)) break;
+          if (!oz_mma_group<S, 1>(P, L, accpar, c, acce, accf)) break;
       }
     }
   } else {
@@ -245,30 +254,39 @@ __global__ void __launch_bounds__(320, 1) oz_gemm_fixed_kernel(const __grid_cons
     uint32_t accpar = 0;
     double sum[64];
     for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
-      const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+      int lt;
+      const GemmArgs &Pg = tile_problem<GROUPED>(a, gt, tile, lt);
+      const int mt = lt / Pg.ntiles, nt = lt % Pg.ntiles;
       const int64_t m0 = (int64_t)mt * 128, n0 = (int64_t)nt * 128;
       named_bar_sync(1, 256);
       if (et < 128) {
         const int64_t n = n0 + et;
-        s_offN[et] = n < a.N ? a.offNC[n] : 0;
-        s_expN[et] = n < a.N ? a.expB[n] : 0;
+        s_offN[et] = n < Pg.N ? Pg.offNC[n] : 0;
+        s_expN[et] = n < Pg.N ? Pg.expB[n] : 0;
+      }
+      if constexpr (GROUPED) {
+        // The tile's problem arguments, staged for the epilogue warps.
+        const int *src = reinterpret_cast<const int *>(&Pg);
+        int *dst = reinterpret_cast<int *>(s_args);
+        for (int w = et; w < (int)(sizeof(GemmArgs) / 4); w += 256) dst[w] = src[w];
       }
       named_bar_sync(1, 256);
+      const GemmArgs &P = GROUPED ? *s_args : a;
       const int64_t i = m0 + 32 * q + lane;
-      const bool row_ok = i < a.M;
-      const int eA = row_ok ? a.expA[i] : 0;
-      const int64_t crow = row_ok ? a.Cbase + a.offMC[a.cplx ? (i >> 1) : i] : 0;
+      const bool row_ok = i < P.M;
+      const int eA = row_ok ? P.expA[i] : 0;
+      const int64_t crow = row_ok ? P.Cbase + P.offMC[P.cplx ? (i >> 1) : i] : 0;
       const bool row_store = row_ok && eA != kNonFinite;
       bool first = true;
-      if (!oz_drain_group<S, 0>(a, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
+      if (!oz_drain_group<S, 0>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
       if constexpr (NG > 1)
-        if (!oz_drain_group<S, 1>(a, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
+        if (!oz_drain_group<S, 1>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         double v[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) v[e] = sum[16 * c + e];
-        store_chunk<double>(a, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+        store_chunk<double>(P, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
       }
     }
   }

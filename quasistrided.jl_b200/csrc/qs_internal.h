@@ -120,6 +120,11 @@ struct qs_plan {
   static constexpr int kProfExec = 256, kProfStages = 5;
   int prof_on = 0, prof_nexec = 0, prof_nstages = 0;
   std::vector<void *> prof_events;
+  // CUDA-graph replay (QS_PLAN_CUDA_GRAPH): graph, instance, capture stream
+  // and the alpha/beta baked into it.
+  void *graph = nullptr, *graph_exec = nullptr, *cap_stream = nullptr;
+  double gal[2] = {0, 0}, gbe[2] = {0, 0};
+  int capturing = 0;
 };
 
 namespace qs {

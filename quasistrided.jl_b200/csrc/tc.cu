@@ -101,9 +101,9 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
 // non-negative doubles the integer order is the value order, and any NaN or
 // Inf sorts above every finite value).  Grid: 32-row blocks x 128-wide K
 // blocks; one atomicMax per row and block.
-__global__ void __launch_bounds__(256) oz_rowmax_kernel(PackArgs a, unsigned long long *rowmax) {
+__device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, unsigned long long *rowmax,
+                                                int64_t r0, int64_t k0) {
   __shared__ double tile[32][129];
-  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 128;
   load_tile<double, 128>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, part = threadIdx.x & 7;  // 8 threads per row
@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(256) oz_rowmax_kernel(PackArgs a, unsigned lon
 // gives digits |d_p| <= 127 with v ~= 2^E * sum_p d_p 254^-p; the error is
 // the tail 254^-s plus one rounding of 254 x per digit.  Rows with a NaN or
 // Inf get exponent kNonFinite, zero digits, and are listed for the fixup.
-__global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigned long long *rowmax) {
+__device__ __forceinline__ void oz_slice_block(const PackArgs &a, const unsigned long long *rowmax,
+                                               int64_t r0, int64_t k0) {
   __shared__ double tile[32][129];
-  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 128;
   load_tile<double, 128>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // 16-byte chunk c of the row
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigne
     frexp(__longlong_as_double((long long)mb), &E);
     E += 1;
   }
-  if (blockIdx.y == 0 && c == 0) {
+  if (k0 == 0 && c == 0) {
     a.exp_out[grow] = E;
     if (bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
   }
@@ -171,9 +171,8 @@ __global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigne
 
 // Split-BF16 planes of one 32-row x 64-element block: hi = bf16(x),
 // lo = bf16(x - hi), x in FP32.
-__global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
+__device__ __forceinline__ void bf16_pack_block(const PackArgs &a, int64_t r0, int64_t k0) {
   __shared__ float tile[32][65];
-  const int64_t r0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 64;
   load_tile<float, 64>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // 8 values per chunk
@@ -192,6 +191,17 @@ __global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
   const int64_t off = panel_tile_base(a, grow, (k0 + c * 8) * 2);
   *reinterpret_cast<uint4 *>(a.panel + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
   *reinterpret_cast<uint4 *>(a.panel + a.plane + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+// One plan: grid (row blocks of 32, K blocks).
+__global__ void __launch_bounds__(256) oz_rowmax_kernel(PackArgs a, unsigned long long *rowmax) {
+  oz_rowmax_block(a, rowmax, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 128);
+}
+__global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigned long long *rowmax) {
+  oz_slice_block(a, rowmax, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 128);
+}
+__global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
+  bf16_pack_block(a, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 64);
 }
 
 // ---------------------------------------------------------------- GEMM ---
@@ -282,6 +292,32 @@ constexpr size_t gemm_smem_bytes() {
          Cfg::BN * (sizeof(int64_t) + sizeof(int32_t));
 }
 
+// The problem table of a grouped launch: tile t of the launch belongs to
+// problem p when tile_start[p] <= t < tile_start[p + 1].  nprob == 0 means a
+// single problem, the kernel's own GemmArgs.
+struct GemmTable {
+  const GemmArgs *tab;
+  const int *tile_start;
+  int nprob;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ const GemmArgs &tile_problem(const GemmArgs &a, const GemmTable &g, int t,
+                                                        int &local) {
+  if (!GROUPED) {
+    local = t;
+    return a;
+  }
+  int lo = 0, hi = g.nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(g.tile_start + mid) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  local = t - __ldg(g.tile_start + lo);
+  return g.tab[lo];
+}
+
 __device__ __forceinline__ int seg_count(const GemmArgs &a, int kind) {
   return kind == KIND_I8 ? a.nslices * a.nkseg : 1;
 }
@@ -312,7 +348,7 @@ __device__ __forceinline__ void seg_krange(const GemmArgs &a, int kind, int g, i
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ GemmArgs a) {
+__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ GemmArgs a, const GemmTable gt) {
   using Cfg = GemmCfg<KIND>;
   constexpr int BN = Cfg::BN, STAGES = Cfg::STAGES;
   constexpr uint32_t A_BYTES = kTileM * kKBytes, B_BYTES = BN * kKBytes;
@@ -349,24 +385,26 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int ntile_total = a.mtiles * a.ntiles;
-  const int nseg = seg_count(a, KIND);
+  const int ntile_total = gt.nprob ? gt.tile_start[gt.nprob] : a.mtiles * a.ntiles;
 
   if (warp == 0) {
     // ---------------------------------------------------- producer ----
     if (lane == 0) {
       uint32_t stage = 0, phase = 0;
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
-        const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+        int lt;
+        const GemmArgs &P = gt.nprob ? tile_problem<true>(a, gt, tile, lt) : tile_problem<false>(a, gt, tile, lt);
+        const int mt = lt / P.ntiles, nt = lt % P.ntiles;
+        const int nseg = seg_count(P, KIND);
         for (int g = 0; g < nseg; ++g) {
           int kb0, kb1;
-          seg_krange(a, KIND, g, kb0, kb1);
-          const int nt_terms = seg_terms(a, KIND, g);
+          seg_krange(P, KIND, g, kb0, kb1);
+          const int nt_terms = seg_terms(P, KIND, g);
           for (int j = 0; j < nt_terms; ++j) {
             int pa, pb;
-            seg_term(a, KIND, g, j, pa, pb);
-            const uint8_t *srcA = a.panelA + pa * a.planeA + ((int64_t)mt * a.kblocks) * A_BYTES;
-            const uint8_t *srcB = a.panelB + pb * a.planeB + ((int64_t)nt * a.kblocks) * B_BYTES;
+            seg_term(P, KIND, g, j, pa, pb);
+            const uint8_t *srcA = P.panelA + pa * P.planeA + ((int64_t)mt * P.kblocks) * A_BYTES;
+            const uint8_t *srcB = P.panelB + pb * P.planeB + ((int64_t)nt * P.kblocks) * B_BYTES;
             for (int kb = kb0; kb < kb1; ++kb) {
               if (!mbar_wait(&empty[stage], phase ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
               mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
@@ -386,14 +424,17 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     if (lane == 0) {
       uint32_t stage = 0, phase = 0, sc = 0;
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+        int lt;
+        const GemmArgs &P = gt.nprob ? tile_problem<true>(a, gt, tile, lt) : tile_problem<false>(a, gt, tile, lt);
+        const int nseg = seg_count(P, KIND);
         for (int g = 0; g < nseg; ++g, ++sc) {
           const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
           if (!mbar_wait(&acce[buf], ap ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
           tc_fence_after();
           const uint32_t d = tmem + buf * BN;
           int kb0, kb1;
-          seg_krange(a, KIND, g, kb0, kb1);
-          const int nt_terms = seg_terms(a, KIND, g);
+          seg_krange(P, KIND, g, kb0, kb1);
+          const int nt_terms = seg_terms(P, KIND, g);
           uint32_t acc = 0;
           for (int j = 0; j < nt_terms; ++j) {
             for (int kb = kb0; kb < kb1; ++kb) {
@@ -426,29 +467,32 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     const uint32_t lane_base = (uint32_t)(32 * q) << 16;
     uint32_t sc = 0;
     for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
-      const int mt = tile / a.ntiles, nt = tile % a.ntiles;
+      int lt;
+      const GemmArgs &P = gt.nprob ? tile_problem<true>(a, gt, tile, lt) : tile_problem<false>(a, gt, tile, lt);
+      const int mt = lt / P.ntiles, nt = lt % P.ntiles;
+      const int nseg = seg_count(P, KIND);
       const int64_t m0 = (int64_t)mt * kTileM, n0 = (int64_t)nt * BN;
       named_bar_sync(1, 128);
       for (int j = et; j < BN; j += 128) {
         int64_t n = n0 + j;
-        s_offN[j] = n < a.N ? a.offNC[n] : 0;
-        s_expN[j] = (KIND == KIND_I8 && n < a.N) ? a.expB[n] : 0;
+        s_offN[j] = n < P.N ? P.offNC[n] : 0;
+        s_expN[j] = (KIND == KIND_I8 && n < P.N) ? P.expB[n] : 0;
       }
       named_bar_sync(1, 128);
       const int64_t i = m0 + 32 * q + lane;  // real (virtual) row
-      const bool row_ok = i < a.M;
-      const int eA = (KIND == KIND_I8 && row_ok) ? a.expA[i] : 0;
-      const int64_t crow = row_ok ? a.Cbase + a.offMC[a.cplx ? (i >> 1) : i] : 0;
+      const bool row_ok = i < P.M;
+      const int eA = (KIND == KIND_I8 && row_ok) ? P.expA[i] : 0;
+      const int64_t crow = row_ok ? P.Cbase + P.offMC[P.cplx ? (i >> 1) : i] : 0;
       const bool row_store = row_ok && eA != kNonFinite;
       for (int g = 0; g < nseg; ++g, ++sc) {
         const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
-        if (!mbar_wait(&accf[buf], ap, abort, a.status, QS_ETIMEOUT)) goto done;
+        if (!mbar_wait(&accf[buf], ap, abort, P.status, QS_ETIMEOUT)) goto done;
         tc_fence_after();
         const bool first = (g == 0), last = (g == nseg - 1);
         const uint32_t tacc = tmem + lane_base + buf * BN;
         const uint32_t tsum = tmem + lane_base + 256;
         double w = 1.0;
-        if (KIND == KIND_I8) w = a.wdiag[g / a.nkseg];
+        if (KIND == KIND_I8) w = P.wdiag[g / P.nkseg];
 #pragma unroll 1
         for (int c = 0; c < BN / 16; ++c) {
           uint32_t dr[16], sr[32];
@@ -474,13 +518,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
               tmem_st16(tsum + 32 * c, sr);
               tmem_st16(tsum + 32 * c + 16, sr + 16);
             } else {
-              store_chunk<double>(a, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+              store_chunk<double>(P, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
             }
           } else {
             float v[16];
 #pragma unroll
             for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(dr[e]);
-            store_chunk<float>(a, v, c, n0, row_store, crow, lane, s_offN, s_expN, 0);
+            store_chunk<float>(P, v, c, n0, row_store, crow, lane, s_offN, s_expN, 0);
           }
         }
         if (KIND == KIND_I8 && !last) tmem_st_wait();
@@ -870,13 +914,13 @@ static OzSched build_oz_sched(int s) {
 // rows; for the 1m layout rows 2i and 2i+1 are both flagged and the even one
 // stands for complex row i.
 template <class T>
-__global__ void oz_fixup_kernel(Operands op, Scalars<T> s, int cplx, const int32_t *rows,
-                                const int32_t *nrows, const int32_t *cols, const int32_t *ncols,
-                                const int32_t *expA) {
+__device__ __forceinline__ void oz_fixup_range(const Operands &op, const Scalars<T> &s, int cplx,
+                                               const int32_t *rows, const int32_t *nrows,
+                                               const int32_t *cols, const int32_t *ncols,
+                                               const int32_t *expA, int64_t first, int64_t stride) {
   const int nr = *nrows, nc = *ncols;
   const int64_t total = (int64_t)nr * op.N + (int64_t)nc * op.M;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t e = first; e < total; e += stride) {
     int64_t i, j;
     if (e < (int64_t)nr * op.N) {
       i = rows[e / op.N];
@@ -901,6 +945,34 @@ __global__ void oz_fixup_kernel(Operands op, Scalars<T> s, int cplx, const int32
     const T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
     store_c<T>(op.C, idx, op.TC, axpby(s, acc, old));
   }
+}
+
+// The fixup of one plan: its operands, scalars and non-finite lists.
+struct FixupJob {
+  Operands op;
+  double alpha[2], beta[2];
+  int beta_case, cplx;
+  const int32_t *rows, *nrows, *cols, *ncols, *expA;
+};
+
+__device__ __forceinline__ void oz_fixup_job(const FixupJob &f, int64_t first, int64_t stride) {
+  if (f.cplx) {
+    Scalars<cplx<double>> s;
+    s.alpha.re = f.alpha[0]; s.alpha.im = f.alpha[1];
+    s.beta.re = f.beta[0]; s.beta.im = f.beta[1];
+    s.beta_case = f.beta_case;
+    oz_fixup_range<cplx<double>>(f.op, s, 1, f.rows, f.nrows, f.cols, f.ncols, f.expA, first, stride);
+  } else {
+    Scalars<double> s;
+    s.alpha = f.alpha[0];
+    s.beta = f.beta[0];
+    s.beta_case = f.beta_case;
+    oz_fixup_range<double>(f.op, s, 0, f.rows, f.nrows, f.cols, f.ncols, f.expA, first, stride);
+  }
+}
+
+__global__ void __launch_bounds__(256) oz_fixup_kernel(const __grid_constant__ FixupJob f) {
+  oz_fixup_job(f, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------- host side ---
@@ -1011,9 +1083,13 @@ int tc_prepare(qs_plan *p) {
                          (int)gemm_smem_bytes<KIND_BF16>());
     cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
-    cudaFuncSetAttribute(oz_gemm_fixed_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<6, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
-    cudaFuncSetAttribute(oz_gemm_fixed_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<7, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     attr_set[0] = attr_set[1] = true;
   }
@@ -1066,6 +1142,68 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   return a;
 }
 
+static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const double *beta,
+                               int beta_case) {
+  const TensorCoreGeom &g = p->tc;
+  const bool oz = p->method == QS_METHOD_OZAKI_I8;
+  GemmArgs a;
+  a.panelA = (const uint8_t *)p->ws.panelA;
+  a.panelB = (const uint8_t *)p->ws.panelB;
+  a.planeA = g.plane_bytes_a;
+  a.planeB = g.plane_bytes_b;
+  a.mtiles = (int)g.mtiles;
+  a.ntiles = (int)g.ntiles;
+  a.kblocks = (int)g.kblocks;
+  a.nslices = g.nslices;
+  a.kseg_blocks = oz ? g.kseg : (int)g.kblocks;
+  a.nkseg = oz ? (int)cdiv(g.kblocks, g.kseg) : 1;
+  a.expA = p->ws.expA;
+  a.expB = p->ws.expB;
+  a.C = p->Cdata;
+  a.Cbase = p->Cbase;
+  a.TC = p->TC;
+  a.offMC = p->ws.offM[1];
+  a.offNC = p->ws.offN[1];
+  a.M = p->M * g.rows_per_elem_a;
+  a.N = p->N;
+  a.cplx = g.kmul == 2;
+  a.alpha_im = alpha[1];
+  a.beta_im = beta[1];
+  a.alpha = alpha[0];
+  a.beta = beta[0];
+  a.beta_case = beta_case;
+  a.status = p->ws.status;
+  for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
+  return a;
+}
+
+static FixupJob make_fixup_job(const qs_plan *p, const double *alpha, const double *beta,
+                               int beta_case) {
+  const TensorCoreGeom &g = p->tc;
+  FixupJob f;
+  Operands &op = f.op;
+  op.A = p->Adata; op.B = p->Bdata; op.C = p->Cdata;
+  op.Abase = p->Abase; op.Bbase = p->Bbase; op.Cbase = p->Cbase;
+  op.TA = p->TA; op.TB = p->TB; op.TC = p->TC;
+  op.conjA = p->conjA; op.conjB = p->conjB;
+  op.offMA = p->ws.offM[0]; op.offMC = p->ws.offM[1];
+  op.offNB = p->ws.offN[0]; op.offNC = p->ws.offN[1];
+  op.offKA = p->ws.offK[0]; op.offKB = p->ws.offK[1];
+  op.M = p->M; op.N = p->N; op.K = p->K;
+  f.alpha[0] = alpha[0]; f.alpha[1] = alpha[1];
+  f.beta[0] = beta[0]; f.beta[1] = beta[1];
+  f.beta_case = beta_case;
+  f.cplx = g.kmul == 2;
+  int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: N][2 counters]
+  int32_t *counters = lists + g.Mp + p->N;
+  f.rows = lists;
+  f.nrows = counters;
+  f.cols = lists + g.Mp;
+  f.ncols = counters + 1;
+  f.expA = p->ws.expA;
+  return f;
+}
+
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
                cudaStream_t st, cudaEvent_t *ev) {
   const TensorCoreGeom &g = p->tc;
@@ -1097,81 +1235,30 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     }
     if (ev) cudaEventRecord(ev[side + 1], st);
   }
-  GemmArgs a;
-  a.panelA = (const uint8_t *)p->ws.panelA;
-  a.panelB = (const uint8_t *)p->ws.panelB;
-  a.planeA = g.plane_bytes_a;
-  a.planeB = g.plane_bytes_b;
-  a.mtiles = (int)g.mtiles;
-  a.ntiles = (int)g.ntiles;
-  a.kblocks = (int)g.kblocks;
-  a.nslices = g.nslices;
-  a.kseg_blocks = oz ? g.kseg : (int)g.kblocks;
-  a.nkseg = oz ? (int)cdiv(g.kblocks, g.kseg) : 1;
-  a.expA = p->ws.expA;
-  a.expB = p->ws.expB;
-  a.C = p->Cdata;
-  a.Cbase = p->Cbase;
-  a.TC = p->TC;
-  a.offMC = p->ws.offM[1];
-  a.offNC = p->ws.offN[1];
-  a.M = p->M * g.rows_per_elem_a;
-  a.N = p->N;
-  a.cplx = g.kmul == 2;
-  a.alpha_im = alpha[1];
-  a.beta_im = beta[1];
-  a.alpha = alpha[0];
-  a.beta = beta[0];
-  a.beta_case = beta_case;
-  a.status = p->ws.status;
-  for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
+  const GemmArgs a = make_gemm_args(p, alpha, beta, beta_case);
   const int tiles = a.mtiles * a.ntiles;
   const int grid = std::min(tiles, num_sms());
   if (oz) {
     if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) {
-      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices == 6) {
-      oz_gemm_fixed_kernel<6><<<grid, 320, oz_smem_bytes(), st>>>(a);
+      oz_gemm_fixed_kernel<6, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices == 7) {
-      oz_gemm_fixed_kernel<7><<<grid, 320, oz_smem_bytes(), st>>>(a);
+      oz_gemm_fixed_kernel<7, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices <= 8) {
       const OzSched sched = build_oz_sched(g.nslices);
       oz_gemm_kernel<<<grid, 320, oz_smem_bytes(), st>>>(a, sched);
     } else {
-      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a);
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     }
   } else {
-    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a);
+    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
   }
   ++launches;
   if (ev) cudaEventRecord(ev[3], st);
   if (oz) {
-    Operands op;
-    op.A = p->Adata; op.B = p->Bdata; op.C = p->Cdata;
-    op.Abase = p->Abase; op.Bbase = p->Bbase; op.Cbase = p->Cbase;
-    op.TA = p->TA; op.TB = p->TB; op.TC = p->TC;
-    op.conjA = p->conjA; op.conjB = p->conjB;
-    op.offMA = p->ws.offM[0]; op.offMC = p->ws.offM[1];
-    op.offNB = p->ws.offN[0]; op.offNC = p->ws.offN[1];
-    op.offKA = p->ws.offK[0]; op.offKB = p->ws.offK[1];
-    op.M = p->M; op.N = p->N; op.K = p->K;
-    int32_t *lists = p->ws.expA + g.Mp + g.Np;
-    int32_t *counters = lists + g.Mp + p->N;
-    if (g.kmul == 2) {
-      Scalars<cplx<double>> sc;
-      sc.alpha.re = alpha[0]; sc.alpha.im = alpha[1];
-      sc.beta.re = beta[0]; sc.beta.im = beta[1];
-      sc.beta_case = beta_case;
-      oz_fixup_kernel<cplx<double>><<<64, 256, 0, st>>>(op, sc, 1, lists, counters, lists + g.Mp,
-                                                        counters + 1, p->ws.expA);
-    } else {
-      Scalars<double> sc;
-      sc.alpha = alpha[0];
-      sc.beta = beta[0];
-      sc.beta_case = beta_case;
-      oz_fixup_kernel<double><<<64, 256, 0, st>>>(op, sc, 0, lists, counters, lists + g.Mp,
-                                                  counters + 1, p->ws.expA);
-    }
+    const FixupJob f = make_fixup_job(p, alpha, beta, beta_case);
+    oz_fixup_kernel<<<64, 256, 0, st>>>(f);
     ++launches;
     if (ev) cudaEventRecord(ev[4], st);
   }
@@ -1186,13 +1273,218 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   return QS_OK;
 }
 
-int tc_execute_grouped(int n, qs_plan *const *plans, const double *alpha, const double *beta,
-                       cudaStream_t st) {
-  for (int i = 0; i < n; ++i) {
-    int rc = qs_execute(plans[i], alpha + 2 * i, beta + 2 * i, (void *)st);
-    if (rc) return rc;
+// ---------------------------------------------------------- grouped ---
+// Many independent plans of one class as one launch per stage: pack (rowmax
+// and slices, or the BF16 planes), the persistent GEMM over a problem table,
+// and the non-finite fixup.  Each plan keeps its own workspace; the launch
+// reads per-problem arguments from device tables.
+
+// One operand side of one problem in a grouped pack launch: blocks
+// [block_start, block_start + gx * kblocks) of the launch.
+struct PackJob {
+  PackArgs pa;
+  unsigned long long *rowmax;  // Ozaki: this side's row-max words
+  int gx;                      // 32-row blocks
+  int block_start;
+};
+
+// A per-plan prep: the row-max words and the non-finite counters to zero.
+struct ZeroJob {
+  unsigned long long *rowmax;
+  int64_t nwords;  // even: Mp + Np
+  int32_t *counters;
+};
+
+__device__ __forceinline__ int pack_job(const PackJob *jobs, int njobs, int b) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].block_start <= b) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int n) {
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    const ZeroJob z = jobs[j];
+    uint4 *w = reinterpret_cast<uint4 *>(z.rowmax);
+    for (int64_t i = threadIdx.x; i < z.nwords / 2; i += blockDim.x) w[i] = make_uint4(0, 0, 0, 0);
+    if (threadIdx.x < 2) z.counters[threadIdx.x] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) oz_rowmax_grouped(const PackJob *jobs, int njobs) {
+  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+  const int lb = blockIdx.x - j.block_start;
+  const PackArgs pa = j.pa;
+  oz_rowmax_block(pa, j.rowmax, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 128);
+}
+
+__global__ void __launch_bounds__(256) oz_slice_grouped(const PackJob *jobs, int njobs) {
+  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+  const int lb = blockIdx.x - j.block_start;
+  const PackArgs pa = j.pa;
+  oz_slice_block(pa, j.rowmax, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 128);
+}
+
+__global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
+  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+  const int lb = blockIdx.x - j.block_start;
+  const PackArgs pa = j.pa;
+  bf16_pack_block(pa, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 64);
+}
+
+// One block per plan (grid-strided); a plan with nothing flagged returns at
+// once.
+__global__ void __launch_bounds__(256) oz_fixup_grouped(const FixupJob *jobs, int n) {
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    const FixupJob &f = jobs[j];
+    if (*f.nrows == 0 && *f.ncols == 0) continue;
+    oz_fixup_job(f, threadIdx.x, blockDim.x);
+  }
+}
+
+int tc_group_class(const qs_plan *p) {
+  if (p->method == QS_METHOD_BF16X3) return TC_CLASS_BF16;
+  if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) return TC_CLASS_I8;
+  if (p->tc.nslices == 6) return TC_CLASS_OZ6;
+  if (p->tc.nslices == 7) return TC_CLASS_OZ7;
+  return TC_CLASS_I8;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const int *bcase) {
+  const int n = (int)g.plans.size();
+  const bool oz = g.cls != TC_CLASS_BF16;
+  std::vector<PackJob> jobs;
+  std::vector<GemmArgs> gemm;
+  std::vector<int> tiles(1, 0);
+  std::vector<ZeroJob> zero;
+  std::vector<FixupJob> fix;
+  int blocks = 0;
+  for (int i = 0; i < n; ++i) {
+    const qs_plan *p = g.plans[i];
+    const TensorCoreGeom &tg = p->tc;
+    const double *al = alpha + 2 * g.idx[i], *be = beta + 2 * g.idx[i];
+    for (int side = 0; side < 2; ++side) {
+      PackJob j;
+      j.pa = pack_args(p, side);
+      j.rowmax = oz ? (unsigned long long *)p->ws.rowmax + (side ? tg.Mp : 0) : nullptr;
+      j.gx = (int)cdiv(j.pa.rows_pad, 32);
+      j.block_start = blocks;
+      const int64_t nb = (int64_t)j.gx * tg.kblocks;
+      if (blocks + nb > INT_MAX) return fail(QS_EINVAL, "ArgumentError: grouped pack launch too large");
+      blocks += (int)nb;
+      jobs.push_back(j);
+    }
+    gemm.push_back(make_gemm_args(p, al, be, bcase[g.idx[i]]));
+    const int64_t t = (int64_t)tiles.back() + (int64_t)tg.mtiles * tg.ntiles;
+    if (t > INT_MAX) return fail(QS_EINVAL, "ArgumentError: grouped GEMM launch too large");
+    tiles.push_back((int)t);
+    if (oz) {
+      ZeroJob z;
+      z.rowmax = (unsigned long long *)p->ws.rowmax;
+      z.nwords = tg.Mp + tg.Np;
+      z.counters = p->ws.expA + tg.Mp + tg.Np + tg.Mp + p->N;
+      zero.push_back(z);
+      fix.push_back(make_fixup_job(p, al, be, bcase[g.idx[i]]));
+    }
+  }
+  g.njobs = (int)jobs.size();
+  g.pack_blocks = blocks;
+  g.tiles = tiles.back();
+  size_t off = 0;
+  g.off_pack = off;
+  off = align_up(off + jobs.size() * sizeof(PackJob), 64);
+  g.off_gemm = off;
+  off = align_up(off + gemm.size() * sizeof(GemmArgs), 64);
+  g.off_tiles = off;
+  off = align_up(off + tiles.size() * sizeof(int), 64);
+  g.off_zero = off;
+  off = align_up(off + zero.size() * sizeof(ZeroJob), 64);
+  g.off_fix = off;
+  off = align_up(off + fix.size() * sizeof(FixupJob), 64);
+  g.image.assign(off, 0);
+  auto put = [&](size_t at, const void *src, size_t bytes) {
+    if (bytes) std::memcpy(g.image.data() + at, src, bytes);
+  };
+  put(g.off_pack, jobs.data(), jobs.size() * sizeof(PackJob));
+  put(g.off_gemm, gemm.data(), gemm.size() * sizeof(GemmArgs));
+  put(g.off_tiles, tiles.data(), tiles.size() * sizeof(int));
+  put(g.off_zero, zero.data(), zero.size() * sizeof(ZeroJob));
+  put(g.off_fix, fix.data(), fix.size() * sizeof(FixupJob));
   return QS_OK;
+}
+
+int tc_group_upload(TcGroup &g, cudaStream_t st) {
+  if (g.dev_bytes < g.image.size()) {
+    if (g.dev) cudaFree(g.dev);
+    g.dev = nullptr;
+    g.dev_bytes = 0;
+    cudaError_t e = cudaMalloc(&g.dev, g.image.size());
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(QS_ENOMEM, "device allocation of a grouped launch's tables failed");
+    }
+    g.dev_bytes = g.image.size();
+  }
+  cudaError_t e = cudaMemcpyAsync(g.dev, g.image.data(), g.image.size(), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemcpyAsync (grouped launch tables)");
+  return QS_OK;
+}
+
+int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
+  const int n = (int)g.plans.size();
+  if (n == 0) return QS_OK;
+  uint8_t *d = (uint8_t *)g.dev;
+  const PackJob *jobs = (const PackJob *)(d + g.off_pack);
+  const GemmArgs *tab = (const GemmArgs *)(d + g.off_gemm);
+  const int *tile_start = (const int *)(d + g.off_tiles);
+  const GemmTable gt{tab, tile_start, n};
+  // The kernel's own GemmArgs: the first problem's (the launch-wide status
+  // word and the table-independent fields).
+  GemmArgs base;
+  std::memcpy(&base, g.image.data() + g.off_gemm, sizeof(GemmArgs));
+  const int grid = std::min(g.tiles, num_sms());
+  int l = 0;
+  if (g.cls == TC_CLASS_BF16) {
+    bf16_pack_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
+    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(base, gt);
+    l = 2;
+  } else {
+    const ZeroJob *zero = (const ZeroJob *)(d + g.off_zero);
+    const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
+    const int pgrid = std::min(n, 4 * num_sms());
+    oz_prep_grouped<<<pgrid, 256, 0, st>>>(zero, n);
+    oz_rowmax_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
+    oz_slice_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
+    if (g.cls == TC_CLASS_OZ6)
+      oz_gemm_fixed_kernel<6, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
+    else if (g.cls == TC_CLASS_OZ7)
+      oz_gemm_fixed_kernel<7, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
+    else
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(base, gt);
+    oz_fixup_grouped<<<pgrid, 256, 0, st>>>(fix, n);
+    l = 5;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::ostringstream s;
+    s << "CUDA error in grouped tensor-core launch: " << cudaGetErrorString(e);
+    return fail(QS_ECUDA, s.str());
+  }
+  count_launches(l);
+  if (launches) *launches += l;
+  return QS_OK;
+}
+
+void tc_group_release(TcGroup &g) {
+  if (g.dev) cudaFree(g.dev);
+  g.dev = nullptr;
+  g.dev_bytes = 0;
+  g.image.clear();
 }
 
 }  // namespace qs

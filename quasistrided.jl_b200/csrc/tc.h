@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "qs_internal.h"
 
 namespace qs {
@@ -17,8 +20,28 @@ int tc_prepare(qs_plan *p);
 // `ev` (nullable) receives an event before the first launch and after each.
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
                cudaStream_t st, cudaEvent_t *ev = nullptr);
-// Many independent plans as one launch per stage.
-int tc_execute_grouped(int n, qs_plan *const *plans, const double *alpha, const double *beta,
-                       cudaStream_t st);
+// Kernel class of a tensor-core plan in a grouped launch: plans of one class
+// share every launch of the class (pack, GEMM, fixup).
+enum { TC_CLASS_OZ6 = 0, TC_CLASS_OZ7 = 1, TC_CLASS_I8 = 2, TC_CLASS_BF16 = 3, TC_NCLASS = 4 };
+int tc_group_class(const qs_plan *p);
+
+// The device tables of one class of a grouped launch: a host image built by
+// tc_group_build and a device copy uploaded by tc_group_upload.
+struct TcGroup {
+  int cls = 0;
+  std::vector<qs_plan *> plans;  // cost-descending
+  std::vector<int> idx;          // position of each plan in the group's alpha/beta arrays
+  std::vector<uint8_t> image;
+  void *dev = nullptr;
+  size_t dev_bytes = 0;
+  size_t off_pack = 0, off_gemm = 0, off_tiles = 0, off_zero = 0, off_fix = 0;
+  int njobs = 0, pack_blocks = 0, tiles = 0;
+};
+// alpha/beta hold 2 doubles per plan of the group, bcase one int per plan.
+int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const int *bcase);
+int tc_group_upload(TcGroup &g, cudaStream_t st);
+// Enqueues the class's launches; adds their count to *launches.
+int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches);
+void tc_group_release(TcGroup &g);
 
 }  // namespace qs
