@@ -172,7 +172,8 @@ def roofline(plan, stage_ms, nexec):
         ms = per.get("gemm_i8")
         peak = 2.0 * peaks["bf16_tflops"]
         note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
-        kernel = "tc_gemm_kernel<KIND_I8>"
+        kernel = (f"oz_gemm_fixed_kernel<{s}, false>" if s in (6, 7) and not plan.per_product_gemm
+                  else "tc_gemm_kernel<KIND_I8>")
     elif plan.method == "bf16x3":
         work = 3 * FLOPS
         ms = per.get("gemm_bf16")
@@ -294,6 +295,111 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+def run_blocks(args):
+    """Uneven blocks of a U(1)-symmetric step: 2000 independent contractions
+    C[x,y,z] = sum A[x,k1,k2,y] * B[k2,z,k1] (alpha = 1, beta = 0), Float64
+    and Float32, as (1) one execute per block from C (the plain launches),
+    (2) a CUDA graph of those launches, (3) grouped persistent launches,
+    (4) a CUDA graph of the grouped launches.  Prints one JSON line."""
+    import torch
+    qs = load_engine()
+    from oracle import oracle as orc
+    wl = __import__(qs.__name__ + ".workloads", fromlist=["u1_blocks"])
+    blocks = wl.u1_blocks(n=args.blocks, seed=20261203, cap=args.block_cap)
+    hist = wl.histogram(blocks)
+    flops = hist["flops"]
+    modes = (("plain", "sequential", False), ("plain_graph", "sequential", True),
+             ("grouped", "persistent", False), ("grouped_graph", "persistent", True))
+    out = {"metric": "aggregate contraction TFLOP/s over uneven blocks (grouped persistent launches)",
+           "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "data": "synthetic (seeded N(0,1) operands)",
+           "config": {"workload": f"u1_blocks_{len(blocks)}", "cap_elements": args.block_cap,
+                      "alpha": 1.0, "beta": 0.0, "l2": "operands larger than L2, no flush"},
+           "histogram": hist, "by_dtype": {}}
+    gen = torch.Generator(device="cuda")
+    for dt_name, tdt, et in (("f64", torch.float64, "Float64"), ("f32", torch.float32, "Float32")):
+        if dt_name not in args.dtypes.split(","):
+            continue
+        gen.manual_seed(7)
+        views, plans = [], []
+        for b in blocks:
+            sa, la = b.a_shape_labels()
+            sb, lb = b.b_shape_labels()
+            sc, lc = b.c_shape_labels()
+            Ad = torch.randn(int(np.prod(sa)), dtype=tdt, device="cuda", generator=gen)
+            Bd = torch.randn(int(np.prod(sb)), dtype=tdt, device="cuda", generator=gen)
+            Cd = torch.zeros(int(np.prod(sc)), dtype=tdt, device="cuda")
+            Av = qs.StridedView(Ad, sa, colmajor_strides(sa), 0)
+            Bv = qs.StridedView(Bd, sb, colmajor_strides(sb), 0)
+            Cv = qs.StridedView(Cd, sc, colmajor_strides(sc), 0)
+            views.append((Av, Bv, Cv, la, lb, lc))
+            plans.append(qs.plan_contract(Cv, Av, la, Bv, lb, lc))
+        torch.cuda.synchronize()
+        n = len(plans)
+        ones, zeros = [1.0] * n, [0.0] * n
+        res = {"methods": {}}
+        for p in plans:
+            res["methods"][p.method] = res["methods"].get(p.method, 0) + 1
+        # Accuracy on a few blocks against the FP64 oracle (grouped result).
+        g = qs.ContractGroup(plans, mode="persistent")
+        g.execute(ones, zeros)
+        torch.cuda.synchronize()
+        errs = []
+        idx = sorted(range(n), key=lambda i: blocks[i].flops)
+        for i in (idx[0], idx[n // 2], idx[-1]):
+            Av, Bv, Cv, la, lb, lc = views[i]
+            Ah = orc.HostView(Av.parent.cpu().numpy().astype(np.float64), Av.size, Av.strides)
+            Bh = orc.HostView(Bv.parent.cpu().numpy().astype(np.float64), Bv.size, Bv.strides)
+            Ch = orc.HostView(np.zeros(Cv.parent.numel()), Cv.size, Cv.strides)
+            orc.brute(Ch, 1.0, Ah, la, Bh, lb, 0.0, lc)
+            got = Cv.parent.cpu().numpy().astype(np.float64)
+            errs.append(float(np.linalg.norm(got - Ch.parent) / max(np.linalg.norm(Ch.parent), 1e-300)))
+        g.release()
+        res["rel_err_max_sampled"] = max(errs)
+        subsets = {}
+        if args.breakdown:
+            for meth in res["methods"]:
+                subsets["grouped_only_" + meth] = [p for p in plans if p.method == meth]
+        run_modes = [m for m in modes if args.modes == "all" or m[0] in args.modes.split(",")]
+        run_modes += [(k, "persistent", False) for k in subsets]
+        for name, mode, graph in run_modes:
+            members = subsets.get(name, plans)
+            ones, zeros = [1.0] * len(members), [0.0] * len(members)
+            g = qs.ContractGroup(members, mode=mode, graph=graph)
+            for _ in range(args.warmup):
+                g.execute(ones, zeros)
+            torch.cuda.synchronize()
+            l0 = qs._abi.lib().qs_launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            for _ in range(args.steps):
+                g.execute(ones, zeros)
+            e1.record()
+            torch.cuda.synchronize()
+            wall = (time.perf_counter() - t0) * 1e3 / args.steps
+            ms = e0.elapsed_time(e1) / args.steps
+            launches = (qs._abi.lib().qs_launch_count() - l0) / args.steps
+            info = g.info()
+            res[name] = {"ms_per_step": ms, "host_ms_per_step": wall, "tflops": flops / (ms * 1e-3) / 1e12,
+                         "kernels_per_step": launches if not graph else info["launches"],
+                         "classes": info["classes"], "tc_plans": info["tc_plans"],
+                         "native_plans": info["native_plans"]}
+            g.release()
+        out["by_dtype"][dt_name] = res
+        for p in plans:
+            p.release()
+        del views, plans
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    f64 = out["by_dtype"].get("f64", {})
+    out["value"] = f64.get("grouped", {}).get("tflops")
+    out["ms_per_step"] = f64.get("grouped", {}).get("ms_per_step")
+    out["dtype"] = "f64"
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,6 +414,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile", action="store_true",
                     help="profiling target: plan, one warm-up execute, --steps executes, exit")
+    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks"],
+                    help="blocks: 2000 uneven U(1) blocks, grouped vs graph vs plain launches")
+    ap.add_argument("--blocks", type=int, default=2000)
+    ap.add_argument("--modes", default="all",
+                    help="blocks: comma list of plain,plain_graph,grouped,grouped_graph (or all)")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="blocks: also time each method's plans as their own grouped launch")
+    ap.add_argument("--dtypes", default="f64,f32")
+    ap.add_argument("--block-cap", type=int, default=1 << 21,
+                    help="max |A|+|B|+|C| elements per block")
     ap.add_argument("--peaks", action="store_true",
                     help="measure cuBLAS int8 (torch._int_mm) and fp64 GEMM throughput, print JSON")
     args = ap.parse_args()
@@ -324,6 +440,9 @@ def main():
         return
     if args.profile:
         run_profile_target(args)
+        return
+    if args.workload == "blocks":
+        run_blocks(args)
         return
 
     import torch

@@ -293,7 +293,9 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     h = ctypes.c_void_p()
     _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))
-    return ContractPlan(h, C, A, B, host_only)
+    plan = ContractPlan(h, C, A, B, host_only)
+    plan.per_product_gemm, plan.cuda_graph = bool(per_product_gemm), bool(cuda_graph)
+    return plan
 
 
 def _stream_ptr(stream) -> Optional[int]:

@@ -42,31 +42,38 @@ __global__ void scale_kernel(Operands op, Scalars<T> s, int mfast) {
 }
 
 // -------------------------------------------------------- native GEMM ----
-// Register-tiled gather GEMM: a CTA computes a BM x BN tile of C; each of
-// its 256 threads owns TM x TN outputs.  A/B tiles are gathered through the
+// Register-tiled gather GEMM: a CTA computes a BM x BN tile of C; its 256
+// threads form an NTY x NTX grid, each owning TM x TN outputs (rows
+// ty + NTY*i, columns tx + NTX*j).  A/B tiles are gathered through the
 // offset tables (coalesced along whichever axis is unit-stride), converted
 // to the compute type with conjugation on load, and double-buffered in
 // shared memory.  The K loop runs over all of K, so beta is applied once.
+// Tile shapes (DirectShape below) follow N: narrow-N problems get tall,
+// narrow tiles instead of padding N to 64.
 
-template <class T, int BM, int BN, int BK>
+template <class T, int BM_, int BN_, int BK_, int TN_>
 struct DirectCfg {
+  static constexpr int BM = BM_, BN = BN_, BK = BK_, TN = TN_;
   static constexpr int kThreads = 256;
-  static constexpr int TM = BM / 16;
-  static constexpr int TN = BN / 16;
+  static constexpr int NTX = BN / TN;
+  static constexpr int NTY = kThreads / NTX;
+  static constexpr int TM = BM / NTY;
   static constexpr int A_PER_THREAD = BM * BK / kThreads;
-  static constexpr int B_PER_THREAD = BN * BK / kThreads;
+  static constexpr int B_PER_THREAD = (BN * BK + kThreads - 1) / kThreads;
+  static_assert(NTX * NTY == kThreads && TM * NTY == BM && TN * NTX == BN, "tile shape");
+  static_assert(A_PER_THREAD * kThreads == BM * BK, "A tile");
 };
 
 // The tile (bx, by) of one problem; the whole CTA calls it.
-template <class T, int BM, int BN, int BK>
+template <class T, class Cfg>
 __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scalars<T> &s,
                                                  int a_mfast, int b_nfast, int64_t bx, int64_t by) {
-  using Cfg = DirectCfg<T, BM, BN, BK>;
-  constexpr int TM = Cfg::TM, TN = Cfg::TN;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+  constexpr int TM = Cfg::TM, TN = Cfg::TN, NTX = Cfg::NTX, NTY = Cfg::NTY;
   __shared__ T As[2][BK][BM];
   __shared__ T Bs[2][BK][BN];
   const int tid = threadIdx.x;
-  const int tx = tid % 16, ty = tid / 16;
+  const int tx = tid % NTX, ty = tid / NTX;
   const int64_t m0 = bx * BM, n0 = by * BN;
 
   T acc[TM][TN];
@@ -83,6 +90,7 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
   auto b_coord = [&](int r, int &nn, int &kk) {
     int e = tid + r * Cfg::kThreads;
     if (b_nfast) { nn = e % BN; kk = e / BN; } else { kk = e % BK; nn = e / BK; }
+    return e < BN * BK;
   };
   auto gather = [&](int64_t k0) {
 #pragma unroll
@@ -97,9 +105,9 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
 #pragma unroll
     for (int r = 0; r < Cfg::B_PER_THREAD; ++r) {
       int nn, kk;
-      b_coord(r, nn, kk);
+      const bool in = b_coord(r, nn, kk);
       int64_t n = n0 + nn, k = k0 + kk;
-      rb[r] = (n < op.N && k < op.K)
+      rb[r] = (in && n < op.N && k < op.K)
                   ? Loader<T>::load(op.B, op.Bbase + op.offNB[n] + op.offKB[k], op.TB, op.conjB)
                   : tzero<T>();
     }
@@ -114,8 +122,7 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
 #pragma unroll
     for (int r = 0; r < Cfg::B_PER_THREAD; ++r) {
       int nn, kk;
-      b_coord(r, nn, kk);
-      Bs[buf][kk][nn] = rb[r];
+      if (b_coord(r, nn, kk)) Bs[buf][kk][nn] = rb[r];
     }
   };
 
@@ -131,9 +138,9 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
     for (int kk = 0; kk < kmax; ++kk) {
       T a[TM], b[TN];
 #pragma unroll
-      for (int i = 0; i < TM; ++i) a[i] = As[cur][kk][ty + 16 * i];
+      for (int i = 0; i < TM; ++i) a[i] = As[cur][kk][ty + NTY * i];
 #pragma unroll
-      for (int j = 0; j < TN; ++j) b[j] = Bs[cur][kk][tx + 16 * j];
+      for (int j = 0; j < TN; ++j) b[j] = Bs[cur][kk][tx + NTX * j];
 #pragma unroll
       for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -145,12 +152,12 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
 
 #pragma unroll
   for (int i = 0; i < TM; ++i) {
-    int64_t m = m0 + ty + 16 * i;
+    int64_t m = m0 + ty + NTY * i;
     if (m >= op.M) continue;
     int64_t cm = op.Cbase + op.offMC[m];
 #pragma unroll
     for (int j = 0; j < TN; ++j) {
-      int64_t n = n0 + tx + 16 * j;
+      int64_t n = n0 + tx + NTX * j;
       if (n >= op.N) continue;
       int64_t idx = cm + op.offNC[n];
       T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
@@ -159,10 +166,30 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
   }
 }
 
-template <class T, int BM, int BN, int BK>
+template <class T, class Cfg>
 __global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T> s, int a_mfast,
                                                           int b_nfast) {
-  direct_gemm_tile<T, BM, BN, BK>(op, s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+  direct_gemm_tile<T, Cfg>(op, s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+}
+
+// Tile shapes: 0 = 64 x 64 (N > 32), 1 = 128 x 32 (16 < N <= 32),
+// 2 = 256 x 16 (N <= 16); complex compute types use 32 x 32 throughout.
+template <class T, int SHAPE, bool CPLX = is_cplx<T>::value>
+struct DirectShape;
+template <class T>
+struct DirectShape<T, 0, false> { using Cfg = DirectCfg<T, 64, 64, 16, 4>; };
+template <class T>
+struct DirectShape<T, 1, false> { using Cfg = DirectCfg<T, 128, 32, 16, 4>; };
+template <class T>
+struct DirectShape<T, 2, false> { using Cfg = DirectCfg<T, 256, 16, 8, 4>; };
+template <class T, int SHAPE>
+struct DirectShape<T, SHAPE, true> { using Cfg = DirectCfg<T, 32, 32, 16, 2>; };
+
+int direct_shape(int T, int64_t N) {
+  if (T == QS_C32 || T == QS_C64) return 0;
+  if (N <= 16) return 2;
+  if (N <= 32) return 1;
+  return 0;
 }
 
 // Grouped: CTA b runs tile b - block_start of the problem whose block range
@@ -177,7 +204,7 @@ struct NativeJob {
   int block_start;
 };
 
-template <class T, int BM, int BN, int BK>
+template <class T, class Cfg>
 __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJob<T> *jobs, int njobs) {
   int lo = 0, hi = njobs - 1;
   const int b = blockIdx.x;
@@ -190,7 +217,7 @@ __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJo
   const int lb = b - j.block_start;
   const Operands op = j.op;
   const Scalars<T> s = j.s;
-  direct_gemm_tile<T, BM, BN, BK>(op, s, j.a_mfast, j.b_nfast, lb % j.gx, lb / j.gx);
+  direct_gemm_tile<T, Cfg>(op, s, j.a_mfast, j.b_nfast, lb % j.gx, lb / j.gx);
 }
 
 // ---------------------------------------------------------------- dot ----
@@ -344,22 +371,33 @@ cudaError_t launch_scale(int T, const Operands &op, const double *beta, int beta
   }
 }
 
-template <class T, int BM, int BN, int BK>
-static cudaError_t launch_direct_t(const Operands &op, const double *alpha, const double *beta,
+template <class T, int SHAPE>
+static cudaError_t launch_direct_s(const Operands &op, const Scalars<T> &s, int a_mfast, int b_nfast,
+                                   cudaStream_t st) {
+  using Cfg = typename DirectShape<T, SHAPE>::Cfg;
+  dim3 grid((unsigned)((op.M + Cfg::BM - 1) / Cfg::BM), (unsigned)((op.N + Cfg::BN - 1) / Cfg::BN));
+  direct_gemm_kernel<T, Cfg><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
+  return cudaGetLastError();
+}
+
+template <class T>
+static cudaError_t launch_direct_t(int Tcode, const Operands &op, const double *alpha, const double *beta,
                                    int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
   auto s = make_scalars<T>(alpha, beta, beta_case);
-  dim3 grid((unsigned)((op.M + BM - 1) / BM), (unsigned)((op.N + BN - 1) / BN));
-  direct_gemm_kernel<T, BM, BN, BK><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
-  return cudaGetLastError();
+  switch (direct_shape(Tcode, op.N)) {
+    case 1: return launch_direct_s<T, 1>(op, s, a_mfast, b_nfast, st);
+    case 2: return launch_direct_s<T, 2>(op, s, a_mfast, b_nfast, st);
+    default: return launch_direct_s<T, 0>(op, s, a_mfast, b_nfast, st);
+  }
 }
 
 cudaError_t launch_direct(int T, const Operands &op, const double *alpha, const double *beta,
                           int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
   switch (T) {
-    case QS_F32: return launch_direct_t<float, 64, 64, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    case QS_F64: return launch_direct_t<double, 64, 64, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    case QS_C32: return launch_direct_t<cplx<float>, 32, 32, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    default: return launch_direct_t<cplx<double>, 32, 32, 16>(op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_F32: return launch_direct_t<float>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_F64: return launch_direct_t<double>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_C32: return launch_direct_t<cplx<float>>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    default: return launch_direct_t<cplx<double>>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
   }
 }
 
@@ -419,15 +457,9 @@ cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const d
   }
 }
 
-// Tile shape per compute type (BM, BN, BK).
-template <class T> struct DirectShape { static constexpr int BM = 64, BN = 64, BK = 16; };
-template <> struct DirectShape<cplx<float>> { static constexpr int BM = 32, BN = 32, BK = 16; };
-template <> struct DirectShape<cplx<double>> { static constexpr int BM = 32, BN = 32, BK = 16; };
-
 template <class T>
 static int native_group_build_t(NativeGroup &g, const Operands *ops, const double *alpha,
                                 const double *beta, const int *bcase) {
-  using Sh = DirectShape<T>;
   const int n = (int)g.plans.size();
   std::vector<NativeJob<T>> jobs(n);
   int64_t blocks = 0;
@@ -438,7 +470,11 @@ static int native_group_build_t(NativeGroup &g, const Operands *ops, const doubl
     j.s = make_scalars<T>(alpha + 2 * k, beta + 2 * k, bcase[k]);
     j.a_mfast = g.plans[i]->a_mfast;
     j.b_nfast = g.plans[i]->b_nfast;
-    const int64_t gx = (j.op.M + Sh::BM - 1) / Sh::BM, gy = (j.op.N + Sh::BN - 1) / Sh::BN;
+    int bm = 64, bn = 64;
+    if (is_complex(g.T)) bm = bn = 32;
+    else if (g.shape == 1) bm = 128, bn = 32;
+    else if (g.shape == 2) bm = 256, bn = 16;
+    const int64_t gx = (j.op.M + bm - 1) / bm, gy = (j.op.N + bn - 1) / bn;
     if (gx > INT32_MAX || blocks + gx * gy > INT32_MAX) return fail(QS_EINVAL, "ArgumentError: grouped launch too large");
     j.gx = (int)gx;
     j.block_start = (int)blocks;
@@ -460,11 +496,19 @@ int native_group_build(NativeGroup &g, const Operands *ops, const double *alpha,
   }
 }
 
+template <class T, int SHAPE>
+static void native_group_launch_s(const NativeGroup &g, cudaStream_t st) {
+  using Cfg = typename DirectShape<T, SHAPE>::Cfg;
+  direct_gemm_grouped_kernel<T, Cfg><<<g.blocks, 256, 0, st>>>((const NativeJob<T> *)g.dev, (int)g.plans.size());
+}
+
 template <class T>
 static cudaError_t native_group_launch_t(const NativeGroup &g, cudaStream_t st) {
-  using Sh = DirectShape<T>;
-  direct_gemm_grouped_kernel<T, Sh::BM, Sh::BN, Sh::BK>
-      <<<g.blocks, 256, 0, st>>>((const NativeJob<T> *)g.dev, (int)g.plans.size());
+  switch (g.shape) {
+    case 1: native_group_launch_s<T, 1>(g, st); break;
+    case 2: native_group_launch_s<T, 2>(g, st); break;
+    default: native_group_launch_s<T, 0>(g, st); break;
+  }
   return cudaGetLastError();
 }
 

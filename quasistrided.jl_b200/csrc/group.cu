@@ -25,12 +25,17 @@ struct qs_group {
   int mode = QS_GROUP_PERSISTENT;
   std::vector<qs_plan *> plans;
   // Persistent mode: the classes and the plans that run on their own.
-  NativeGroup native[4];  // by compute type QS_F32..QS_C64
+  NativeGroup native[12];  // by compute type QS_F32..QS_C64 x tile shape
   TcGroup tc[TC_NCLASS];
   std::vector<int> single;
   bool built = false;
   std::vector<double> alpha, beta;  // values the tables/graph hold
   int launches = 0;
+  // Persistent mode: side streams that run the classes concurrently (fork
+  // and join through events on the caller's stream).
+  static constexpr int kSide = 4;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork = nullptr, join[kSide] = {};
   // Graph mode.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -77,7 +82,7 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
   release_tables(g);
   const int n = (int)g->plans.size();
   std::vector<int> bcase(n);
-  std::vector<std::vector<int>> nat(4), tcm(TC_NCLASS);
+  std::vector<std::vector<int>> nat(12), tcm(TC_NCLASS);
   for (int i = 0; i < n; ++i) {
     qs_plan *p = g->plans[i];
     const int acase = scalar_case(p->T, alpha + 2 * i);
@@ -86,7 +91,7 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
     if (acase == 0 || p->path != QS_PATH_NEST) {
       g->single.push_back(i);
     } else if (p->method == QS_METHOD_NATIVE) {
-      nat[p->T - QS_F32].push_back(i);
+      nat[3 * (p->T - QS_F32) + direct_shape(p->T, p->N)].push_back(i);
     } else {
       tcm[tc_group_class(p)].push_back(i);
     }
@@ -97,11 +102,12 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
     });
   };
   int rc;
-  for (int t = 0; t < 4; ++t) {
+  for (int t = 0; t < 12; ++t) {
     if (nat[t].empty()) continue;
     by_cost(nat[t]);
     NativeGroup &c = g->native[t];
-    c.T = QS_F32 + t;
+    c.T = QS_F32 + t / 3;
+    c.shape = t % 3;
     std::vector<Operands> ops;
     for (int i : nat[t]) {
       c.plans.push_back(g->plans[i]);
@@ -150,6 +156,18 @@ int execute_member(qs_plan *p, const double *alpha, const double *beta, cudaStre
   return rc;
 }
 
+int ensure_side_streams(qs_group *g) {
+  if (g->fork) return QS_OK;
+  cudaError_t e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+  for (int i = 0; e == cudaSuccess && i < qs_group::kSide; ++i) {
+    e = cudaStreamCreateWithFlags(&g->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming);
+  }
+  return e == cudaSuccess ? QS_OK : gfail(e, "stream/event creation");
+}
+
+// Singles on the caller's stream, then each class on a side stream (the
+// classes are independent: the plans write disjoint C), joined back.
 int launch_persistent(qs_group *g, const double *alpha, const double *beta, cudaStream_t st) {
   int launches = 0;
   for (int i : g->single) {
@@ -158,17 +176,37 @@ int launch_persistent(qs_group *g, const double *alpha, const double *beta, cuda
     if (rc) return rc;
     launches += (int)(qs_launch_count() - before);
   }
+  int rc = ensure_side_streams(g);
+  if (rc) return rc;
+  cudaError_t e = cudaEventRecord(g->fork, st);
+  if (e != cudaSuccess) return gfail(e, "cudaEventRecord");
+  bool used[qs_group::kSide] = {};
+  int next = 0;
+  auto pick = [&]() -> cudaStream_t {
+    const int i = next++ % qs_group::kSide;
+    if (!used[i]) {
+      cudaStreamWaitEvent(g->side[i], g->fork, 0);
+      used[i] = true;
+    }
+    return g->side[i];
+  };
+  // Tensor-core classes first: they are the longest.
+  for (auto &c : g->tc) {
+    if (c.plans.empty()) continue;
+    if ((rc = tc_group_launch(c, pick(), &launches))) return rc;
+  }
   for (auto &c : g->native) {
     if (c.plans.empty()) continue;
-    cudaError_t e = native_group_launch(c, st);
+    e = native_group_launch(c, pick());
     if (e != cudaSuccess) return gfail(e, "grouped gather-GEMM launch");
     count_launches(1);
     ++launches;
   }
-  for (auto &c : g->tc) {
-    if (c.plans.empty()) continue;
-    int rc = tc_group_launch(c, st, &launches);
-    if (rc) return rc;
+  for (int i = 0; i < qs_group::kSide; ++i) {
+    if (!used[i]) continue;
+    e = cudaEventRecord(g->join[i], g->side[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, g->join[i], 0);
+    if (e != cudaSuccess) return gfail(e, "stream join");
   }
   g->launches = launches;
   return QS_OK;
@@ -315,6 +353,11 @@ int qs_group_destroy(qs_group *g) {
   release_graph(g);
   release_tables(g);
   if (g->cap_stream) cudaStreamDestroy(g->cap_stream);
+  for (int i = 0; i < qs_group::kSide; ++i) {
+    if (g->side[i]) cudaStreamDestroy(g->side[i]);
+    if (g->join[i]) cudaEventDestroy(g->join[i]);
+  }
+  if (g->fork) cudaEventDestroy(g->fork);
   delete g;
   return QS_OK;
 }

@@ -82,8 +82,50 @@ __device__ __forceinline__ int64_t panel_tile_base(const PackArgs &a, int64_t ro
 
 // A tile of 32 rows x KT K values of X, converted to the compute type, into
 // smem, coalesced along whichever of rows / K is X's unit-stride axis.
+// Real operands stored as S: each thread keeps the offset of its fixed row
+// (or K index) in a register and issues all of its loads independently.
+template <class T, class S, int KT>
+__device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, int64_t k0,
+                                               T (*tile)[KT + 1]) {
+  const int tid = threadIdx.x;
+  constexpr int PER = 32 * KT / 256;
+  const S *X = static_cast<const S *>(a.X) + a.Xbase;
+  if (a.rfast) {
+    const int rr = tid & 31, kb = tid >> 5;
+    const int64_t r = r0 + rr;
+    const bool rok = r < a.rows;
+    const int64_t ro = rok ? __ldg(a.offR + r) : 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int kk = kb + 8 * i;
+      const int64_t k = k0 + kk;
+      const bool ok = rok && k < a.K;
+      const int64_t ko = ok ? __ldg(a.offK + k) : 0;
+      tile[rr][kk] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+    }
+  } else {
+    constexpr int RSTEP = 256 / KT;
+    const int kk = tid % KT, rb = tid / KT;
+    const int64_t k = k0 + kk;
+    const bool kok = k < a.K;
+    const int64_t ko = kok ? __ldg(a.offK + k) : 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int rr = rb + RSTEP * i;
+      const int64_t r = r0 + rr;
+      const bool ok = kok && r < a.rows;
+      const int64_t ro = ok ? __ldg(a.offR + r) : 0;
+      tile[rr][kk] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+    }
+  }
+}
+
 template <class T, int KT>
 __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t k0, T (*tile)[KT + 1]) {
+  if (a.cmode == 0) {
+    if (a.TX == QS_F64) return load_tile_real<T, double, KT>(a, r0, k0, tile);
+    if (a.TX == QS_F32) return load_tile_real<T, float, KT>(a, r0, k0, tile);
+  }
   const int tid = threadIdx.x;
   constexpr int PER = 32 * KT / 256;
 #pragma unroll 8

@@ -95,6 +95,25 @@ def test_native_real_f64_bitwise_equals_scalar_kernel_order(qs, orc):
         assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("MKN", [(600, 150, 8), (500, 77, 16), (700, 200, 29), (300, 64, 33),
+                                 (257, 300, 17)])
+@pytest.mark.parametrize("b_nfast", [False, True])
+def test_native_narrow_n_tiles_bitwise(qs, orc, MKN, b_nfast):
+    # The narrow-N tile shapes (256 x 16, 128 x 32) keep the ascending-K
+    # muladd order: bitwise equal to the oracle, for B stored K-fast or N-fast.
+    Ma, Ka, Na = MKN
+    rng = np.random.default_rng(Ma + Na)
+    A = colmajor_pair(qs, rng, (Ma, Ka), "Float64")
+    C = colmajor_pair(qs, rng, (Ma, Na), "Float64")
+    if b_nfast:
+        B = colmajor_pair(qs, rng, (Na, Ka), "Float64")
+        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (3, 2), 0.7, (1, 3), method="native")
+    else:
+        B = colmajor_pair(qs, rng, (Ka, Na), "Float64")
+        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native")
+    assert np.array_equal(got, ref)
+
+
 def test_permuted_zero_and_negative_strides_sliced_c(qs, orc):
     # test/execution/test_nest.jl:76-92
     rng = np.random.default_rng(11)
