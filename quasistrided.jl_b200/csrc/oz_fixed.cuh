@@ -218,7 +218,8 @@ __global__ void __launch_bounds__(320, 1)
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
         int lt;
         const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
-        const int mt = lt / P.ntiles, nt = lt % P.ntiles;
+        int mt, nt;
+        tile_coords(lt, P.mtiles, P.ntiles, mt, nt);
         c.planeA = P.planeA;
         c.planeB = P.planeB;
         const uint8_t *tileA = P.panelA + (int64_t)mt * P.kblocks * TILE;
@@ -256,7 +257,8 @@ __global__ void __launch_bounds__(320, 1)
     for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
       int lt;
       const GemmArgs &Pg = tile_problem<GROUPED>(a, gt, tile, lt);
-      const int mt = lt / Pg.ntiles, nt = lt % Pg.ntiles;
+      int mt, nt;
+      tile_coords(lt, Pg.mtiles, Pg.ntiles, mt, nt);
       const int64_t m0 = (int64_t)mt * 128, n0 = (int64_t)nt * 128;
       named_bar_sync(1, 256);
       if (et < 128) {
@@ -277,15 +279,19 @@ __global__ void __launch_bounds__(320, 1)
       const int eA = row_ok ? P.expA[i] : 0;
       const int64_t crow = row_ok ? P.Cbase + P.offMC[P.cplx ? (i >> 1) : i] : 0;
       const bool row_store = row_ok && eA != kNonFinite;
+      if (row_store && (!P.cplx || (lane & 1) == 0)) prefetch_c_row(P, crow, s_offN, 64 * h, 64, n0);
       bool first = true;
       if (!oz_drain_group<S, 0>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
       if constexpr (NG > 1)
         if (!oz_drain_group<S, 1>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
-#pragma unroll
+      // One copy of the store code for the four chunks (c is a runtime
+      // index; the sums are picked with selects, not local memory).
+#pragma unroll 1
       for (int c = 0; c < 4; ++c) {
         double v[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) v[e] = sum[16 * c + e];
+        for (int e = 0; e < 16; ++e)
+          v[e] = c == 0 ? sum[e] : c == 1 ? sum[16 + e] : c == 2 ? sum[32 + e] : sum[48 + e];
         store_chunk<double>(P, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
       }
     }

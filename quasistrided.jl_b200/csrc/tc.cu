@@ -36,6 +36,15 @@ constexpr int kTileM = 128;     // UMMA M
 constexpr int kKBytes = 128;    // bytes of K per panel tile (one swizzle row)
 constexpr int kNonFinite = INT_MIN;
 
+// x * 2^e.  When 2^e is a normal double the product is one multiplication
+// by an exactly built power of two (exact, or rounded once if the result is
+// subnormal), which is ldexp's result; other e take ldexp.
+__device__ __noinline__ double scale2_wide(double x, int e) { return ldexp(x, e); }
+__device__ __forceinline__ double scale2(double x, int e) {
+  if (e >= -1022 && e <= 1023) return x * __longlong_as_double((long long)(e + 1023) << 52);
+  return scale2_wide(x, e);
+}
+
 // ------------------------------------------------------------- packing ---
 
 struct PackArgs {
@@ -194,7 +203,7 @@ __device__ __forceinline__ void oz_slice_block(const PackArgs &a, const unsigned
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) {
     const double v = tile[row][c * 16 + kk];
-    x[kk] = (bad || !mb) ? 0.0 : ldexp(v, -E);
+    x[kk] = (bad || !mb) ? 0.0 : scale2(v, -E);
   }
   const int64_t off = panel_tile_base(a, grow, k0 + c * 16);
   for (int p = 0; p < a.nslices; ++p) {
@@ -275,42 +284,137 @@ struct GemmArgs {
 // in the compute precision R.  Ozaki values are rescaled by 2^(eA + eB) first.
 // Complex (1m): lanes 2l and 2l+1 hold Re and Im of one complex element; the
 // pair is joined with a shuffle and the even lane stores it.
+// Any C eltype, real or complex (1m lane pairs).  Not inlined: the
+// epilogue runs it once per chunk and tile, and its code would otherwise be
+// copied into every call site.
+template <class R>
+__device__ __noinline__ void store_chunk_any(const GemmArgs &a, const R *v, int c, int64_t n0,
+                                             bool row_store, int64_t crow, int lane,
+                                             const int64_t *s_offN, const int32_t *s_expN, int eA) {
+  constexpr int kNF = INT_MIN;
+  constexpr int G = 2;  // old C values in flight per thread (register budget)
+  auto prep = [&](int e, R &x, int64_t &idx) -> bool {
+    const int jj = 16 * c + e;
+    const int eB = s_expN[jj];
+    const bool finite = eA != kNF && eB != kNF;
+    x = v[e];
+    if (sizeof(R) == 8 && finite) x = (R)scale2((double)x, eA + eB);
+    idx = crow + s_offN[jj];
+    return row_store && n0 + jj < a.N && finite;
+  };
+  if (a.cplx) {
+    Scalars<cplx<R>> s;
+    s.alpha.re = (R)a.alpha; s.alpha.im = (R)a.alpha_im;
+    s.beta.re = (R)a.beta; s.beta.im = (R)a.beta_im;
+    s.beta_case = a.beta_case;
+#pragma unroll
+    for (int e0 = 0; e0 < 16; e0 += G) {
+      cplx<R> old[G];
+#pragma unroll
+      for (int e = 0; e < G; ++e) {
+        R x;
+        int64_t idx;
+        const bool ok = prep(e0 + e, x, idx) && (lane & 1) == 0;
+        old[e] = (ok && a.beta_case != 0) ? load_c<cplx<R>>(a.C, idx, a.TC) : tzero<cplx<R>>();
+      }
+#pragma unroll
+      for (int e = 0; e < G; ++e) {
+        R x;
+        int64_t idx;
+        const bool ok = prep(e0 + e, x, idx);
+        const R other = __shfl_xor_sync(0xffffffffu, x, 1);
+        if (ok && (lane & 1) == 0) {
+          cplx<R> r;
+          r.re = x;
+          r.im = other;
+          store_c<cplx<R>>(a.C, idx, a.TC, axpby(s, r, old[e]));
+        }
+      }
+    }
+  } else {
+    Scalars<R> s;
+    s.alpha = (R)a.alpha;
+    s.beta = (R)a.beta;
+    s.beta_case = a.beta_case;
+#pragma unroll
+    for (int e0 = 0; e0 < 16; e0 += G) {
+      R old[G];
+#pragma unroll
+      for (int e = 0; e < G; ++e) {
+        R x;
+        int64_t idx;
+        const bool ok = prep(e0 + e, x, idx);
+        old[e] = (ok && a.beta_case != 0) ? load_c<R>(a.C, idx, a.TC) : (R)0;
+      }
+#pragma unroll
+      for (int e = 0; e < G; ++e) {
+        R x;
+        int64_t idx;
+        if (prep(e0 + e, x, idx)) store_c<R>(a.C, idx, a.TC, axpby(s, x, old[e]));
+      }
+    }
+  }
+}
+
+// Real FP64 C: the compact path.  Old C values are loaded G at a time
+// before their stores, so the loads overlap.
+__device__ __forceinline__ void store_chunk_f64(const GemmArgs &a, const double (&v)[16], int c,
+                                                int64_t n0, bool row_store, int64_t crow,
+                                                const int64_t *s_offN, const int32_t *s_expN,
+                                                int eA) {
+  constexpr int kNF = INT_MIN;
+  constexpr int G = 4;
+  double *C = static_cast<double *>(a.C);
+  const double al = a.alpha, be = a.beta;
+  const int bc = a.beta_case;
+#pragma unroll
+  for (int e0 = 0; e0 < 16; e0 += G) {
+    double old[G];
+#pragma unroll
+    for (int e = 0; e < G; ++e) {
+      const int jj = 16 * c + e0 + e;
+      const bool ok = row_store && n0 + jj < a.N && s_expN[jj] != kNF;
+      old[e] = (ok && bc != 0) ? C[crow + s_offN[jj]] : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < G; ++e) {
+      const int jj = 16 * c + e0 + e;
+      const int eB = s_expN[jj];
+      if (!row_store || n0 + jj >= a.N || eB == kNF) continue;
+      const double x = scale2(v[e0 + e], eA + eB);
+      double r;
+      if (bc == 0) r = al * x;
+      else if (bc == 1) r = fma(al, x, old[e]);
+      else r = fma(al, x, be * old[e]);
+      C[crow + s_offN[jj]] = r;
+    }
+  }
+}
+
 template <class R>
 __device__ __forceinline__ void store_chunk(const GemmArgs &a, const R (&v)[16], int c, int64_t n0,
                                             bool row_store, int64_t crow, int lane,
                                             const int64_t *s_offN, const int32_t *s_expN, int eA) {
-  constexpr int kNF = INT_MIN;
-#pragma unroll
-  for (int e = 0; e < 16; ++e) {
-    const int jj = 16 * c + e;
-    const int64_t n = n0 + jj;
-    const int eB = s_expN[jj];
-    const bool finite = eA != kNF && eB != kNF;
-    R val = v[e];
-    if (sizeof(R) == 8 && finite) val = (R)ldexp((double)val, eA + eB);
-    const bool ok = row_store && n < a.N && finite;
-    const int64_t idx = crow + s_offN[jj];
-    if (a.cplx) {
-      const R other = __shfl_xor_sync(0xffffffffu, val, 1);
-      if (ok && (lane & 1) == 0) {
-        Scalars<cplx<R>> s;
-        s.alpha.re = (R)a.alpha; s.alpha.im = (R)a.alpha_im;
-        s.beta.re = (R)a.beta; s.beta.im = (R)a.beta_im;
-        s.beta_case = a.beta_case;
-        cplx<R> r;
-        r.re = val;
-        r.im = other;
-        const cplx<R> old = a.beta_case == 0 ? tzero<cplx<R>>() : load_c<cplx<R>>(a.C, idx, a.TC);
-        store_c<cplx<R>>(a.C, idx, a.TC, axpby(s, r, old));
-      }
-    } else if (ok) {
-      Scalars<R> s;
-      s.alpha = (R)a.alpha;
-      s.beta = (R)a.beta;
-      s.beta_case = a.beta_case;
-      const R old = a.beta_case == 0 ? (R)0 : load_c<R>(a.C, idx, a.TC);
-      store_c<R>(a.C, idx, a.TC, axpby(s, val, old));
+  if constexpr (sizeof(R) == 8) {
+    if (!a.cplx && a.TC == QS_F64) {
+      store_chunk_f64(a, v, c, n0, row_store, crow, s_offN, s_expN, eA);
+      return;
     }
+  }
+  store_chunk_any<R>(a, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+}
+
+// L2 prefetch of the C elements this thread will read back in its final
+// store (beta != 0): issued when the tile starts, long before the store.
+__device__ __forceinline__ void prefetch_c_row(const GemmArgs &a, int64_t crow, const int64_t *s_offN,
+                                               int j0, int nj, int64_t n0) {
+  if (a.beta_case == 0) return;
+  const int es = (a.TC == QS_F32) ? 4 : (a.TC == QS_C64 ? 16 : 8);
+  const char *base = static_cast<const char *>(a.C);
+  for (int j = j0; j < j0 + nj; ++j) {
+    if (n0 + j >= a.N) break;
+    const char *p = base + (crow + s_offN[j]) * es;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
   }
 }
 
@@ -861,11 +965,16 @@ struct OzFixedSched {
   };
   int ngroups;
   Grp g[2];
+  // The last group takes the top four diagonals (they need every slice of
+  // A and B anyway); the first group the rest.  For s = 6 that is {0, 1}
+  // (4 tile loads, 3 products) and {2..5} (12 loads, 18 products) per K
+  // block.
   constexpr OzFixedSched() : ngroups(S > 4 ? 2 : 1), g{} {
+    const int split = S > 4 ? S - 4 : 0;
     for (int gi = 0; gi < ngroups; ++gi) {
       Grp &G = g[gi];
-      G.t0 = gi == 0 ? 0 : 4;
-      G.t1 = gi == 0 ? (S - 1 < 3 ? S - 1 : 3) : (S - 1 < 7 ? S - 1 : 7);
+      G.t0 = gi == 0 ? 0 : split;
+      G.t1 = (ngroups == 1 || gi == 1) ? S - 1 : split - 1;
       int idxA[16] = {}, idxB[16] = {}, last[kOzMaxLoads] = {};
       for (int x = 0; x < 16; ++x) idxA[x] = idxB[x] = -1;
       for (int l = 0; l < kOzMaxLoads; ++l) G.first_use[l] = -1;
@@ -898,6 +1007,19 @@ struct OzFixedSched {
     }
   }
 };
+
+// Tile t of a problem -> (mt, nt), in bands of kBandM m-tiles: within a band
+// the n-tiles advance slowest, so the CTAs of one wave share a few A panels
+// and a band's worth of B panels instead of every B panel.
+constexpr int kBandM = 16;
+__device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int &mt, int &nt) {
+  const int per_band = kBandM * ntiles;
+  const int band = t / per_band, r = t - band * per_band;
+  const int m0 = band * kBandM;
+  const int bm = mtiles - m0 < kBandM ? mtiles - m0 : kBandM;
+  mt = m0 + r % bm;
+  nt = r / bm;
+}
 
 // Ring slot and phase parity of load l of a block whose first load has
 // global index L (l < 2 * kOzSlots).

@@ -91,16 +91,34 @@ def test_ozaki_persistent_tiles_and_reuse(qs, orc):
     assert np.array_equal(C.device_parent(), first)
 
 
-def test_ozaki_long_k_segments(qs, orc):
-    # K beyond one INT32-exact segment (148 K blocks at 7 slices).
+@pytest.mark.parametrize("slices", [0, 8])
+def test_ozaki_long_k_segments(qs, orc, slices):
+    # K beyond one INT32-exact segment (148 K blocks at 7 slices); slices=0
+    # takes the default for this K (7, the fixed-schedule kernel).
     rng = np.random.default_rng(10)
     M, K, N = 128, 20000, 128
     A = uniform_pair(qs, rng, (M, K))
     B = uniform_pair(qs, rng, (K, N))
     C = colmajor_pair(qs, rng, (M, N), "Float64")
     got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), method="ozaki",
-                              ozaki_slices=8, precision=1)
+                              ozaki_slices=slices, precision=1)
+    assert plan.ozaki_slices == (7 if slices == 0 else slices)
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+@pytest.mark.parametrize("slices,tol", [(5, 1e-10), (6, TOL64), (7, TOL64)])
+def test_ozaki_slice_counts(qs, orc, slices, tol):
+    # Each schedule: s = 5 ({0}, {1..4}), 6 ({0, 1}, {2..5}), 7 ({0..2}, {3..6});
+    # 5 slices are below the 1e-13 target and checked at their own accuracy.
+    rng = np.random.default_rng(20 + slices)
+    M, K, N = 300, 500, 260
+    A = uniform_pair(qs, rng, (M, K))
+    B = uniform_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="ozaki",
+                              ozaki_slices=slices, precision=1)
+    assert plan.ozaki_slices == slices
+    assert rel_fro(got, ref) <= tol, rel_fro(got, ref)
 
 
 def test_ozaki_nonfinite_rows_and_columns(qs, orc):
