@@ -171,6 +171,10 @@ __global__ void __launch_bounds__(320, 1)
     oz_gemm_fixed_kernel(const __grid_constant__ GemmArgs a, const GemmTable gt) {
   constexpr uint32_t TILE = 128 * 128;
   constexpr int NG = kOzSched<S>.ngroups;
+  // The last group (the top diagonals: most products, longest) runs first
+  // in every tile, so a tile's final store overlaps the next tile's long
+  // group instead of stalling the short one.
+  constexpr int kG1 = NG - 1, kG2 = 0;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t *slots = smem;
@@ -224,9 +228,9 @@ __global__ void __launch_bounds__(320, 1)
         c.planeB = P.planeB;
         const uint8_t *tileA = P.panelA + (int64_t)mt * P.kblocks * TILE;
         const uint8_t *tileB = P.panelB + (int64_t)nt * P.kblocks * TILE;
-        if (!oz_produce_group<S, 0>(P, L, c, tileA, tileB)) break;
+        if (!oz_produce_group<S, kG1>(P, L, c, tileA, tileB)) break;
         if constexpr (NG > 1)
-          if (!oz_produce_group<S, 1>(P, L, c, tileA, tileB)) break;
+          if (!oz_produce_group<S, kG2>(P, L, c, tileA, tileB)) break;
       }
     }
   } else if (warp == 1) {
@@ -242,9 +246,9 @@ __global__ void __launch_bounds__(320, 1)
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
         int lt;
         const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
-        if (!oz_mma_group<S, 0>(P, L, accpar, c, acce, accf)) break;
+        if (!oz_mma_group<S, kG1>(P, L, accpar, c, acce, accf)) break;
         if constexpr (NG > 1)
-          if (!oz_mma_group<S, 1>(P, L, accpar, c, acce, accf)) break;
+          if (!oz_mma_group<S, kG2>(P, L, accpar, c, acce, accf)) break;
       }
     }
   } else {
@@ -281,18 +285,29 @@ __global__ void __launch_bounds__(320, 1)
       const bool row_store = row_ok && eA != kNonFinite;
       if (row_store && (!P.cplx || (lane & 1) == 0)) prefetch_c_row(P, crow, s_offN, 64 * h, 64, n0);
       bool first = true;
-      if (!oz_drain_group<S, 0>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
+      if (!oz_drain_group<S, kG1>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
       if constexpr (NG > 1)
-        if (!oz_drain_group<S, 1>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
-      // One copy of the store code for the four chunks (c is a runtime
-      // index; the sums are picked with selects, not local memory).
+        if (!oz_drain_group<S, kG2>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
+      // One copy of the store code per C kind for the four chunks (c is a
+      // runtime index; the sums are picked with selects, not local memory).
+      if (store_is_f64(P)) {
 #pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
-        double v[16];
+        for (int c = 0; c < 4; ++c) {
+          double v[16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e)
-          v[e] = c == 0 ? sum[e] : c == 1 ? sum[16 + e] : c == 2 ? sum[32 + e] : sum[48 + e];
-        store_chunk<double>(P, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+          for (int e = 0; e < 16; ++e)
+            v[e] = c == 0 ? sum[e] : c == 1 ? sum[16 + e] : c == 2 ? sum[32 + e] : sum[48 + e];
+          store_chunk_f64(P, v, 4 * h + c, n0, row_store, crow, s_offN, s_expN, eA);
+        }
+      } else {
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+          double v[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e)
+            v[e] = c == 0 ? sum[e] : c == 1 ? sum[16 + e] : c == 2 ? sum[32 + e] : sum[48 + e];
+          store_chunk_any<double>(P, v, 4 * h + c, n0, row_store, crow, lane, s_offN, s_expN, eA);
+        }
       }
     }
   }

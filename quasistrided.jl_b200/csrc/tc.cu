@@ -91,6 +91,16 @@ __device__ __forceinline__ int64_t panel_tile_base(const PackArgs &a, int64_t ro
 
 // A tile of 32 rows x KT K values of X, converted to the compute type, into
 // smem, coalesced along whichever of rows / K is X's unit-stride axis.
+// Column skew of the pack tiles: element k of a row sits at column
+// tcol(k), which rotates each group of W = KT/8 columns by its group index.
+// The readers take W consecutive columns per thread, eight threads per row;
+// without the skew those eight threads hit one bank.
+template <int KT>
+__device__ __forceinline__ int tcol(int k) {
+  constexpr int W = KT / 8;
+  return (k & ~(W - 1)) | ((k + k / W) & (W - 1));
+}
+
 // Real operands stored as S: each thread keeps the offset of its fixed row
 // (or K index) in a register and issues all of its loads independently.
 template <class T, class S, int KT>
@@ -110,7 +120,7 @@ __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, in
       const int64_t k = k0 + kk;
       const bool ok = rok && k < a.K;
       const int64_t ko = ok ? __ldg(a.offK + k) : 0;
-      tile[rr][kk] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+      tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
     }
   } else {
     constexpr int RSTEP = 256 / KT;
@@ -124,7 +134,7 @@ __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, in
       const int64_t r = r0 + rr;
       const bool ok = kok && r < a.rows;
       const int64_t ro = ok ? __ldg(a.offR + r) : 0;
-      tile[rr][kk] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+      tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
     }
   }
 }
@@ -144,7 +154,7 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
     int64_t r = r0 + rr, k = k0 + kk;
     T v = (T)0;
     if (r < a.rows && k < a.K) v = virtual_elem<T>(a, r, k);
-    tile[rr][kk] = v;
+    tile[rr][tcol<KT>(kk)] = v;
   }
 }
 
@@ -161,7 +171,7 @@ __device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, unsigned long
   unsigned long long m = 0;
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) {
-    unsigned long long b = (unsigned long long)__double_as_longlong(fabs(tile[row][part * 16 + kk]));
+    unsigned long long b = (unsigned long long)__double_as_longlong(fabs(tile[row][tcol<128>(part * 16 + kk)]));
     m = b > m ? b : m;
   }
 #pragma unroll
@@ -202,7 +212,7 @@ __device__ __forceinline__ void oz_slice_block(const PackArgs &a, const unsigned
   double x[16];
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) {
-    const double v = tile[row][c * 16 + kk];
+    const double v = tile[row][tcol<128>(c * 16 + kk)];
     x[kk] = (bad || !mb) ? 0.0 : scale2(v, -E);
   }
   const int64_t off = panel_tile_base(a, grow, k0 + c * 16);
@@ -232,7 +242,7 @@ __device__ __forceinline__ void bf16_pack_block(const PackArgs &a, int64_t r0, i
   uint32_t hw[4], lw[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const float x0 = tile[row][c * 8 + 2 * q], x1 = tile[row][c * 8 + 2 * q + 1];
+    const float x0 = tile[row][tcol<64>(c * 8 + 2 * q)], x1 = tile[row][tcol<64>(c * 8 + 2 * q + 1)];
     const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
     const __nv_bfloat16 l0 = __float2bfloat16_rn(x0 - __bfloat162float(h0));
     const __nv_bfloat16 l1 = __float2bfloat16_rn(x1 - __bfloat162float(h1));
@@ -284,13 +294,11 @@ struct GemmArgs {
 // in the compute precision R.  Ozaki values are rescaled by 2^(eA + eB) first.
 // Complex (1m): lanes 2l and 2l+1 hold Re and Im of one complex element; the
 // pair is joined with a shuffle and the even lane stores it.
-// Any C eltype, real or complex (1m lane pairs).  Not inlined: the
-// epilogue runs it once per chunk and tile, and its code would otherwise be
-// copied into every call site.
+// Any C eltype, real or complex (1m lane pairs).
 template <class R>
-__device__ __noinline__ void store_chunk_any(const GemmArgs &a, const R *v, int c, int64_t n0,
-                                             bool row_store, int64_t crow, int lane,
-                                             const int64_t *s_offN, const int32_t *s_expN, int eA) {
+__device__ __forceinline__ void store_chunk_any(const GemmArgs &a, const R (&v)[16], int c, int64_t n0,
+                                                bool row_store, int64_t crow, int lane,
+                                                const int64_t *s_offN, const int32_t *s_expN, int eA) {
   constexpr int kNF = INT_MIN;
   constexpr int G = 2;  // old C values in flight per thread (register budget)
   auto prep = [&](int e, R &x, int64_t &idx) -> bool {
@@ -391,12 +399,15 @@ __device__ __forceinline__ void store_chunk_f64(const GemmArgs &a, const double 
   }
 }
 
+// Real FP64 C takes the compact path.
+__device__ __forceinline__ bool store_is_f64(const GemmArgs &a) { return !a.cplx && a.TC == QS_F64; }
+
 template <class R>
 __device__ __forceinline__ void store_chunk(const GemmArgs &a, const R (&v)[16], int c, int64_t n0,
                                             bool row_store, int64_t crow, int lane,
                                             const int64_t *s_offN, const int32_t *s_expN, int eA) {
   if constexpr (sizeof(R) == 8) {
-    if (!a.cplx && a.TC == QS_F64) {
+    if (store_is_f64(a)) {
       store_chunk_f64(a, v, c, n0, row_store, crow, s_offN, s_expN, eA);
       return;
     }
