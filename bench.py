@@ -400,6 +400,97 @@ def run_blocks(args):
     print(json.dumps(out), flush=True)
 
 
+def run_serving(args):
+    """Mixed request stream served with continuous batching vs one request at
+    a time, at several Poisson arrival rates.  Prints one JSON line."""
+    import torch
+    qs = load_engine()
+    wl = __import__(qs.__name__ + ".workloads", fromlist=["serving_stream"])
+    sv = __import__(qs.__name__ + ".serving", fromlist=["ContractionServer"])
+    tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+           np.dtype(np.complex128): torch.complex128}
+    pool_elems = 1 << 26
+    pool = wl.pool_arrays(pool_elems, seed=11,
+                          allocate=lambda n, dt: torch.empty(n, dtype=tdt[np.dtype(dt)], pin_memory=True).numpy())
+
+    def requests(specs):
+        out = []
+        for sp in specs:
+            buf = pool[np.dtype(sp["dtype"])]
+            A = sp["resident"] or wl.colmajor_view(buf, sp["shapeA"], 0)
+            nB = int(np.prod(sp["shapeB"]))
+            B = wl.colmajor_view(buf, sp["shapeB"], pool_elems - nB)
+            r = sv.ContractRequest(A, sp["indA"], B, sp["indB"], sp["indC"], alpha=sp["alpha"],
+                                   beta=sp["beta"], dtype=sp["dtype"], tag=sp["family"])
+            if sp["beta"] != 0:
+                sa = sp["shapeA"]
+                dims = dict(zip(sp["indA"], sa))
+                dims.update(zip(sp["indB"], sp["shapeB"]))
+                sc = tuple(dims[l] for l in sp["indC"])
+                r.C0 = wl.colmajor_view(buf, sc, 0)
+            out.append(r)
+        return out
+
+    rates = [float(x) for x in args.rates.split(",")]
+    result = {"metric": "served p50/p99 latency (ms) and aggregate TFLOP/s, mixed contraction stream",
+              "unit": "ms", "n_gpus": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+              "dtype": "mixed f32/f64/c64", "data": "synthetic (seeded N(0,1) pools)",
+              "config": {"workload": f"serving_{args.requests}_requests", "hbm_budget_gb": args.budget_gb,
+                         "families": "matmul, permuted4, mps steps, u1 block, random rank-2..6 pairs",
+                         "reuse": 0.3, "eltypes": "f32/f64/c64 40/40/20"},
+              "rates": []}
+    # One backend (its device and pinned arenas are allocated once); its plan
+    # cache is cleared before every run so no run inherits another's plans.
+    be = sv.DeviceBackend(qs, grouped=True, device_arena_bytes=int(args.arena_gb * (1 << 30)),
+                          host_arena_bytes=int(args.host_arena_gb * (1 << 30)))
+    for rate in rates:
+        specs, offsets, residents = wl.serving_stream(args.requests, rate, seed=int(rate) + 7,
+                                                      pool_elems=pool_elems)
+        row = {"rate_per_s": rate}
+        for mode in ("batched", "sequential"):
+            be.clear_plan_cache()
+            be.timing.clear()
+            be.tick_gpu_ms.clear()
+            be.fallbacks.clear()
+            # the client takes each result as it completes and hands the
+            # pinned buffer back
+            consume = sv.ContractRequest.release_result
+            srv = sv.ContractionServer(be, hbm_budget_bytes=int(args.budget_gb * (1 << 30)),
+                                       max_tick_flops=args.tick_flops, on_done=consume)
+            for key, (shape, dt) in residents.items():
+                srv.put_resident(key, wl.colmajor_view(pool[np.dtype(dt)], shape, 0))
+            # warm-up: the first requests of the stream, untimed
+            warm = requests(specs[:min(10, len(specs))])
+            for r in warm:
+                srv.submit(r)
+            srv.drain()
+            reqs = requests(specs)
+            torch.cuda.synchronize()
+            if mode == "batched":
+                makespan = srv.replay(reqs, offsets)
+            else:
+                makespan = sv.serve_sequential(be, reqs, offsets, on_done=consume)
+            flops = sum(r.flops(be.shape_of) for r in reqs)
+            st = srv.stats(reqs)
+            row[mode] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                         "makespan_s": makespan, "tflops": flops / makespan / 1e12,
+                         "ticks": srv.ticks_launched if mode == "batched" else len(reqs),
+                         "peak_budget_gb": srv.peak_used / (1 << 30), "errors": st["errors"],
+                         "tick_flops": args.tick_flops if mode == "batched" else None,
+                         "host_s": {k: round(v, 4) for k, v in be.timing.items()},
+                         "tick_gpu_ms_sum": round(sum(be.tick_gpu_ms), 2),
+                         "tick_gpu_ms_max": round(max(be.tick_gpu_ms), 2) if be.tick_gpu_ms else None,
+                         "arena_fallbacks": dict(be.fallbacks)}
+            for key in residents:
+                srv.drop_resident(key)
+            del srv
+            torch.cuda.synchronize()
+        result["rates"].append(row)
+    top = result["rates"][-1]["batched"]
+    result["value"] = top["p99_ms"]
+    print(json.dumps(result), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,7 +506,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile", action="store_true",
                     help="profiling target: plan, one warm-up execute, --steps executes, exit")
-    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks"],
+    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks", "serving"],
                     help="blocks: 2000 uneven U(1) blocks, grouped vs graph vs plain launches")
     ap.add_argument("--blocks", type=int, default=2000)
     ap.add_argument("--modes", default="all",
@@ -423,6 +514,12 @@ def main():
     ap.add_argument("--breakdown", action="store_true",
                     help="blocks: also time each method's plans as their own grouped launch")
     ap.add_argument("--dtypes", default="f64,f32")
+    ap.add_argument("--rates", default="100,1000,10000,100000", help="serving: Poisson arrival rates (1/s)")
+    ap.add_argument("--requests", type=int, default=300, help="serving: requests per rate")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="serving: HBM admission budget")
+    ap.add_argument("--arena-gb", type=float, default=64.0, help="serving: device arena for request buffers")
+    ap.add_argument("--host-arena-gb", type=float, default=24.0, help="serving: pinned host arena")
+    ap.add_argument("--tick-flops", type=float, default=2e11, help="serving: work per tick (flops)")
     ap.add_argument("--block-cap", type=int, default=1 << 21,
                     help="max |A|+|B|+|C| elements per block")
     ap.add_argument("--peaks", action="store_true",
@@ -444,6 +541,9 @@ def main():
         return
     if args.workload == "blocks":
         run_blocks(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
 
     import torch

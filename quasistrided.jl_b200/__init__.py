@@ -45,6 +45,10 @@ _DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
 _OPS = ("identity", "conj", "transpose", "adjoint")
 
 
+def _layout_of(v) -> tuple:
+    return (tuple(v.size), tuple(v.strides), int(v.offset), int(v.parent.numel()), v.dtype, v.op)
+
+
 def _eltype(dtype: torch.dtype) -> int:
     try:
         return _DTYPE_TO_QS[dtype]
@@ -185,6 +189,7 @@ class ContractPlan:
     def __init__(self, handle, C, A, B, host_only):
         self._h = handle
         self.C, self.A, self.B = C, A, B
+        self._layout = {"A": _layout_of(A), "B": _layout_of(B), "C": _layout_of(C)}
         self.host_only = host_only
         info = _abi.qs_plan_info()
         _abi.check(_abi.lib().qs_plan_get_info(handle, ctypes.byref(info)))
@@ -205,6 +210,29 @@ class ContractPlan:
     @property
     def Cstorage(self) -> torch.Tensor:
         return self.C.parent
+
+    def rebind(self, A: Optional[StridedView] = None, B: Optional[StridedView] = None,
+               C: Optional[StridedView] = None) -> None:
+        """Point the plan at new storage with the same layout (size, strides,
+        offset, parent length, eltype and op as at plan time); qs_plan_rebind."""
+        def same(new, name):
+            if new is None:
+                if getattr(self, name) is None:
+                    raise ArgumentError(f"rebind: {name} has no storage bound")
+                return None
+            if _layout_of(new) != self._layout[name]:
+                raise ArgumentError(f"rebind: {name} differs in layout from the planned view")
+            return ctypes.c_void_p(new.parent.data_ptr())
+        pa, pb, pc = same(A, "A"), same(B, "B"), same(C, "C")
+        _abi.check(_abi.lib().qs_plan_rebind(self._h, pa, pb, pc))
+        self.A = A if A is not None else self.A
+        self.B = B if B is not None else self.B
+        self.C = C if C is not None else self.C
+
+    def detach_storage(self) -> None:
+        """Drop the plan's references to its operands (their memory may then
+        be freed); the plan executes again only after ``rebind``."""
+        self.A = self.B = self.C = None
 
     def release(self) -> None:
         if self._h:
@@ -313,6 +341,8 @@ def execute(plan: ContractPlan, alpha, beta, stream=None) -> torch.Tensor:
     """
     if plan._h is None:
         raise ArgumentError("plan has been released")
+    if plan.C is None or plan.A is None or plan.B is None:
+        raise ArgumentError("plan has no storage bound (detached): rebind it first")
     a, b = _scalar(alpha), _scalar(beta)
     s = None if plan.host_only else _stream_ptr(stream)
     _abi.check(_abi.lib().qs_execute(plan._h, a, b, s))

@@ -27,6 +27,67 @@ using namespace qs;
 namespace qs {
 static std::atomic<int64_t> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+static cudaStream_t setup_stream(cudaError_t *err) {
+  thread_local cudaStream_t s = nullptr;
+  thread_local int dev = -1;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (!s || dev != cur) {
+    *err = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    dev = cur;
+  }
+  return s;
+}
+
+int setup_copy(void *dst, const void *src, size_t bytes, int to_device) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemcpyAsync(dst, src, bytes, to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return (int)e;
+}
+
+int device_alloc(void **p, size_t bytes) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  if (e != cudaSuccess) return (int)e;
+  thread_local int pool_dev = -1;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (pool_dev != cur) {
+    // Keep freed pool memory mapped instead of returning it at every sync.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, cur) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pool_dev = cur;
+  }
+  e = cudaMallocAsync(p, bytes, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return (int)e;
+}
+
+void device_free_all(std::vector<void *> &ptrs) {
+  if (ptrs.empty()) return;
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  cudaDeviceSynchronize();
+  for (void *q : ptrs) cudaFreeAsync(q, s);
+  cudaStreamSynchronize(s);
+  ptrs.clear();
+}
+
+int setup_zero(void *dst, size_t bytes) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemsetAsync(dst, 0, bytes, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return (int)e;
+}
 }  // namespace qs
 
 namespace qs {
@@ -77,15 +138,14 @@ int cuda_fail(cudaError_t e, const char *what) {
 }
 
 void free_workspace(qs_plan *p) {
-  for (void *q : p->ws.owned) cudaFree(q);
-  p->ws.owned.clear();
+  device_free_all(p->ws.owned);
   p->ws = Workspace{};
 }
 
 int ws_alloc(qs_plan *p, void **out, size_t bytes) {
   *out = nullptr;
   if (bytes == 0) return QS_OK;
-  cudaError_t e = cudaMalloc(out, bytes);
+  cudaError_t e = (cudaError_t)device_alloc(out, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     std::ostringstream s;
@@ -108,8 +168,8 @@ int upload_offsets(qs_plan *p, const Group &g, int64_t **dst) {
   void *d;
   int rc = ws_alloc(p, &d, 2 * n * sizeof(int64_t));
   if (rc) return rc;
-  cudaError_t e = cudaMemcpy(d, h.data(), 2 * n * sizeof(int64_t), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (offset tables)");
+  cudaError_t e = (cudaError_t)setup_copy(d, h.data(), 2 * n * sizeof(int64_t), 1);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (offset tables)");
   dst[0] = (int64_t *)d;
   dst[1] = (int64_t *)d + n;
   return QS_OK;
@@ -363,10 +423,10 @@ int qs_plan_check_status(qs_plan *p, void *stream) {
   cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
   int32_t word = 0;
-  e = cudaMemcpy(&word, p->ws.status, sizeof(word), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (status)");
+  e = (cudaError_t)setup_copy(&word, p->ws.status, sizeof(word), 0);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (status)");
   if (word != 0) {
-    cudaMemset(p->ws.status, 0, sizeof(int32_t));
+    setup_zero(p->ws.status, sizeof(int32_t));
     return fail(QS_ETIMEOUT, "a bounded device wait gave up (tensor-core kernel aborted)");
   }
   return QS_OK;
@@ -441,6 +501,7 @@ int qs_plan_rebind(qs_plan *p, void *A_data, void *B_data, void *C_data) {
   if (a) p->Adata = a;
   if (b) p->Bdata = b;
   if (C_data) p->Cdata = C_data;
+  destroy_graph(p);  // a captured graph holds the old pointers
   return QS_OK;
 }
 

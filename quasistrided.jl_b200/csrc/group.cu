@@ -36,6 +36,11 @@ struct qs_group {
   static constexpr int kSide = 4;
   cudaStream_t side[kSide] = {};
   cudaEvent_t fork = nullptr, join[kSide] = {};
+  // Stream-ordered release of the device tables: `last_use` is recorded on
+  // the caller's stream after every execute; frees go on `rel` after it.
+  cudaStream_t rel = nullptr;
+  cudaEvent_t last_use = nullptr;
+  bool used_since_build = false;
   // Graph mode.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -52,16 +57,33 @@ int gfail(cudaError_t e, const char *what) {
 }
 
 void release_tables(qs_group *g) {
+  if (g->rel && g->used_since_build) cudaStreamWaitEvent(g->rel, g->last_use, 0);
   for (auto &c : g->native) {
-    if (c.dev) cudaFree(c.dev);
+    if (c.dev) cudaFreeAsync(c.dev, g->rel);
     c = NativeGroup{};
   }
   for (auto &c : g->tc) {
-    tc_group_release(c);
+    tc_group_release(c, g->rel);
     c = TcGroup{};
   }
   g->single.clear();
   g->built = false;
+  g->used_since_build = false;
+}
+
+int ensure_release_stream(qs_group *g) {
+  if (g->rel) return QS_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&g->rel, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->last_use, cudaEventDisableTiming);
+  return e == cudaSuccess ? QS_OK : gfail(e, "stream/event creation");
+}
+
+// After launches on `st` that read the current tables.
+int mark_use(qs_group *g, cudaStream_t st) {
+  cudaError_t e = cudaEventRecord(g->last_use, st);
+  if (e != cudaSuccess) return gfail(e, "cudaEventRecord");
+  g->used_since_build = true;
+  return QS_OK;
 }
 
 void release_graph(qs_group *g) {
@@ -79,6 +101,8 @@ int64_t plan_cost(const qs_plan *p) {
 
 // Class membership, device tables and their upload for the given scalars.
 int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStream_t st) {
+  int rc0 = ensure_release_stream(g);
+  if (rc0) return rc0;
   release_tables(g);
   const int n = (int)g->plans.size();
   std::vector<int> bcase(n);
@@ -115,7 +139,7 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
       ops.push_back(make_operands(g->plans[i]));
     }
     if ((rc = native_group_build(c, ops.data(), alpha, beta, bcase.data()))) return rc;
-    cudaError_t e = cudaMalloc(&c.dev, c.image.size());
+    cudaError_t e = cudaMallocAsync(&c.dev, c.image.size(), st);
     if (e != cudaSuccess) {
       cudaGetLastError();
       c.dev = nullptr;
@@ -282,7 +306,9 @@ int qs_group_execute(qs_group *g, const double *alpha, const double *beta, void 
       int rc = build_tables(g, alpha, beta, st);
       if (rc) return rc;
     }
-    return launch(g, alpha, beta, st);
+    int rc = launch(g, alpha, beta, st);
+    if (rc) return rc;
+    return g->built ? mark_use(g, st) : QS_OK;
   }
   if (!g->graph_exec || !same) {
     release_graph(g);
@@ -322,7 +348,7 @@ int qs_group_execute(qs_group *g, const double *alpha, const double *beta, void 
   }
   cudaError_t e = cudaGraphLaunch(g->graph_exec, st);
   if (e != cudaSuccess) return gfail(e, "cudaGraphLaunch");
-  return QS_OK;
+  return g->built ? mark_use(g, st) : QS_OK;
 }
 
 int qs_group_get_info(const qs_group *g, qs_group_info *info) {
@@ -352,6 +378,8 @@ int qs_group_destroy(qs_group *g) {
   if (!g->plans.empty()) cudaSetDevice(g->plans[0]->device);
   release_graph(g);
   release_tables(g);
+  if (g->rel) cudaStreamDestroy(g->rel);  // its frees still run after the device work
+  if (g->last_use) cudaEventDestroy(g->last_use);
   if (g->cap_stream) cudaStreamDestroy(g->cap_stream);
   for (int i = 0; i < qs_group::kSide; ++i) {
     if (g->side[i]) cudaStreamDestroy(g->side[i]);

@@ -128,6 +128,19 @@ struct qs_plan {
 };
 
 namespace qs {
+// Plan-time device copies and clears, on a private non-blocking stream of the
+// calling thread (never the legacy default stream, which would serialize
+// planning with work in flight on other streams); both wait for completion.
+// Return a cudaError_t code.
+int setup_copy(void *dst, const void *src, size_t bytes, int to_device);
+int setup_zero(void *dst, size_t bytes);
+// Plan workspace: stream-ordered allocation on the setup stream (from the
+// device's default pool, which keeps freed memory cached), so planning
+// never waits for kernels in flight.  Freeing synchronizes the device first:
+// the plan's last executes may still be running on any stream.
+int device_alloc(void **p, size_t bytes);
+void device_free_all(std::vector<void *> &ptrs);
+
 // planner.cpp
 int plan_host(qs_plan *p, const qs_view *C, const qs_view *A,
               const int64_t *indA, const qs_view *B, const int64_t *indB,

@@ -1212,7 +1212,7 @@ void tc_geometry(qs_plan *p) {
 
 static int tc_alloc(qs_plan *p, void **out, size_t bytes) {
   *out = nullptr;
-  cudaError_t e = cudaMalloc(out, bytes);
+  cudaError_t e = (cudaError_t)device_alloc(out, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     std::ostringstream s;
@@ -1240,14 +1240,14 @@ int tc_prepare(qs_plan *p) {
     int32_t *b = (int32_t *)q;
     p->ws.expA = b;
     p->ws.expB = b + g.Mp;
-    if (cudaMemset(q, 0, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
+    if (setup_zero(q, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
     p->ws.status = b + n - 1;
     // row/column max bit patterns, cleared per execute
     if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
     p->ws.rowmax = q;
   } else {
     if ((rc = tc_alloc(p, &q, 4 * sizeof(int32_t)))) return rc;
-    if (cudaMemset(q, 0, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemset");
+    if (setup_zero(q, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
     p->ws.status = (int32_t *)q;
   }
   static bool attr_set[2] = {false, false};
@@ -1593,19 +1593,19 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   return QS_OK;
 }
 
+// Stream-ordered: the tables are allocated on the build stream and freed on
+// the group's release stream after their last use (tc_group_release), so
+// building and dropping groups never synchronizes the device.
 int tc_group_upload(TcGroup &g, cudaStream_t st) {
-  if (g.dev_bytes < g.image.size()) {
-    if (g.dev) cudaFree(g.dev);
+  if (g.dev) return fail(QS_EINVAL, "internal: grouped tables already uploaded");
+  cudaError_t e = cudaMallocAsync(&g.dev, g.image.size(), st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
     g.dev = nullptr;
-    g.dev_bytes = 0;
-    cudaError_t e = cudaMalloc(&g.dev, g.image.size());
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(QS_ENOMEM, "device allocation of a grouped launch's tables failed");
-    }
-    g.dev_bytes = g.image.size();
+    return fail(QS_ENOMEM, "device allocation of a grouped launch's tables failed");
   }
-  cudaError_t e = cudaMemcpyAsync(g.dev, g.image.data(), g.image.size(), cudaMemcpyHostToDevice, st);
+  g.dev_bytes = g.image.size();
+  e = cudaMemcpyAsync(g.dev, g.image.data(), g.image.size(), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemcpyAsync (grouped launch tables)");
   return QS_OK;
 }
@@ -1655,8 +1655,8 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
   return QS_OK;
 }
 
-void tc_group_release(TcGroup &g) {
-  if (g.dev) cudaFree(g.dev);
+void tc_group_release(TcGroup &g, cudaStream_t rel) {
+  if (g.dev) cudaFreeAsync(g.dev, rel);
   g.dev = nullptr;
   g.dev_bytes = 0;
   g.image.clear();

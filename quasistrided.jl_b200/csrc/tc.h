@@ -42,6 +42,7 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
 int tc_group_upload(TcGroup &g, cudaStream_t st);
 // Enqueues the class's launches; adds their count to *launches.
 int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches);
-void tc_group_release(TcGroup &g);
+// Frees the tables on `rel`, a stream already ordered after their last use.
+void tc_group_release(TcGroup &g, cudaStream_t rel);
 
 }  // namespace qs
