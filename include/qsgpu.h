@@ -129,6 +129,8 @@ typedef struct qs_plan_options {
   int32_t ozaki_slices;    /* 0 = chosen from K for 1e-13; else 2..10 */
   int32_t complex_mode;    /* QS_CPLX_*; 0 = default for the method */
   int32_t flags;           /* QS_PLAN_* */
+  int32_t native_tile;     /* gather-GEMM tile: 0 = by N; 1 = 64x64, 2 = 128x32,
+                              3 = 256x16 (real compute types; the autotuner's knob) */
 } qs_plan_options;
 
 typedef struct qs_plan_info {
@@ -145,6 +147,9 @@ typedef struct qs_plan_info {
   int32_t bounds_ok; /* 0 when qs_execute would return QS_EBOUNDS */
   int64_t m_labels[16], n_labels[16], k_labels[16]; /* group label order */
   int64_t workspace_bytes;
+  int32_t stride_class;  /* bit 0: A's M map unit-stride, bit 1: B's N map,
+                            bit 2: C's M map (the autotuner's stride class) */
+  int32_t native_tile;   /* gather-GEMM tile in use (1..3 as in the options) */
 } qs_plan_info;
 
 typedef struct qs_plan qs_plan;

@@ -206,6 +206,8 @@ class ContractPlan:
         self.k_labels = tuple(info.k_labels[:info.k_rank])
         self.bounds_ok = bool(info.bounds_ok)
         self.workspace_bytes = info.workspace_bytes
+        self.stride_class = info.stride_class
+        self.native_tile = info.native_tile
 
     @property
     def Cstorage(self) -> torch.Tensor:
@@ -297,7 +299,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                   n_block=None, allocator=None, accumulator=None,
                   path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
                   complex_mode=None, host_only=False, per_product_gemm=False,
-                  cuda_graph=False) -> ContractPlan:
+                  cuda_graph=False, native_tile=0) -> ContractPlan:
     """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
 
     Throws ArgumentError / DimensionMismatch on invalid input, before any
@@ -318,6 +320,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
                  ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph)
+    o.native_tile = int(native_tile)
     h = ctypes.c_void_p()
     _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))

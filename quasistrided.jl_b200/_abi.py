@@ -66,6 +66,7 @@ class qs_plan_options(ctypes.Structure):
         ("ozaki_slices", ctypes.c_int32),
         ("complex_mode", ctypes.c_int32),
         ("flags", ctypes.c_int32),
+        ("native_tile", ctypes.c_int32),
     ]
 
 
@@ -90,6 +91,8 @@ class qs_plan_info(ctypes.Structure):
         ("n_labels", ctypes.c_int64 * 16),
         ("k_labels", ctypes.c_int64 * 16),
         ("workspace_bytes", ctypes.c_int64),
+        ("stride_class", ctypes.c_int32),
+        ("native_tile", ctypes.c_int32),
     ]
 
 

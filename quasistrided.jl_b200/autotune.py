@@ -1,0 +1,194 @@
+"""Autotuner for the contraction path, with an on-disk cache.
+
+For a contraction it picks the plan options that run fastest on this GPU
+while meeting the accuracy target:
+
+* method: the gather GEMM (``native``) or the tensor-core path (``ozaki`` for
+  Float64/ComplexF64, ``bf16x3`` for Float32/ComplexF32);
+* the Ozaki GEMM kernel (grouped diagonals, or one product per stage);
+* the gather GEMM's tile shape (64x64, 128x32, 256x16; real types);
+* the Ozaki slice count: the default for K, raised while a probe on random
+  data of the problem's layout misses the target (relative Frobenius error
+  against the FP64 gather result: 1e-13 for Float64, 1e-5 for Float32).
+
+Candidates run on scratch operands with the problem's exact layout (sizes,
+strides, offsets, parent lengths, eltypes), never on the caller's data.  The
+choice is keyed by (M/N/K class, stride class, eltypes, accumulator, conj)
+and stored as JSON, so a later process on the same device reuses it.  This
+replaces the reference's analytical cache-blocking model
+(src/planning/blocking.jl): on the device the knobs are kernel choices, and
+they are measured rather than modelled.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import statistics
+import tempfile
+from typing import Callable, Optional
+
+CACHE_VERSION = 1
+
+
+def default_cache_path() -> str:
+    env = os.environ.get("QS_AUTOTUNE_CACHE")
+    if env:
+        return env
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "quasistrided_b200", "autotune.json")
+
+
+def size_class(n: int) -> int:
+    """log2 bucket of an extent (0 for empty or 1)."""
+    return 0 if n <= 1 else int(math.ceil(math.log2(n)))
+
+
+class Autotuner:
+    """``options(C, A, indA, B, indB, indC, **kw)`` returns plan_contract
+    keyword arguments; ``plan(...)`` plans with them.  ``measure`` (tests)
+    replaces the GPU timing: measure(candidate_options) -> (ms, rel_err)."""
+
+    def __init__(self, qs, path: Optional[str] = None, reps: int = 5,
+                 measure: Optional[Callable] = None, device_name: Optional[str] = None):
+        self.qs = qs
+        self.path = path or default_cache_path()
+        self.reps = reps
+        self._measure = measure
+        self.device_name = device_name
+        self.hits = 0
+        self.misses = 0
+        self.entries = {}
+        self._load()
+
+    # ----------------------------------------------------------- cache ---
+    def _device(self) -> str:
+        if self.device_name is None:
+            import torch
+            self.device_name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+        return self.device_name
+
+    def _load(self) -> None:
+        try:
+            with open(self.path) as f:
+                d = json.load(f)
+            if d.get("version") == CACHE_VERSION:
+                self.entries = d.get("entries", {})
+        except (OSError, ValueError):
+            self.entries = {}
+
+    def save(self) -> None:
+        os.makedirs(os.path.dirname(os.path.abspath(self.path)), exist_ok=True)
+        fd, tmp = tempfile.mkstemp(dir=os.path.dirname(os.path.abspath(self.path)), suffix=".tmp")
+        with os.fdopen(fd, "w") as f:
+            json.dump({"version": CACHE_VERSION, "entries": self.entries}, f, indent=1, sort_keys=True)
+        os.replace(tmp, self.path)
+
+    def key(self, hp, C, A, B, accumulator, conjA, conjB) -> str:
+        """Problem class of a host-only plan."""
+        return "|".join(str(x) for x in (
+            self._device(), hp.compute_type, str(A.dtype), str(B.dtype), str(C.dtype),
+            accumulator or "-", int(conjA), int(conjB), hp.path,
+            size_class(hp.m_length), size_class(hp.n_length), size_class(hp.k_length), hp.stride_class))
+
+    # ------------------------------------------------------ candidates ---
+    @staticmethod
+    def candidates(hp) -> list:
+        real = not hp.compute_type.startswith("Complex")
+        dbl = hp.compute_type in ("Float64", "ComplexF64")
+        out = []
+        if real:
+            out += [{"method": "native", "native_tile": t} for t in (1, 2, 3)]
+        else:
+            out.append({"method": "native"})
+        if dbl:
+            out.append({"method": "ozaki"})
+            out.append({"method": "ozaki", "per_product_gemm": True})
+        else:
+            out.append({"method": "bf16x3"})
+        return out
+
+    # -------------------------------------------------------- measure ---
+    def _scratch(self, v):
+        import torch
+        g = torch.Generator(device=v.parent.device)
+        g.manual_seed(1234)
+        p = torch.randn(v.parent.numel(), dtype=v.parent.dtype, device=v.parent.device, generator=g)
+        return self.qs.StridedView(p, v.size, v.strides, v.offset, v.op)
+
+    def _run(self, opts, C, A, indA, B, indB, indC, kw, ref_store=None):
+        """(median ms of `reps` executes, rel. error vs the FP64 gather
+        result) of one candidate on scratch operands."""
+        import torch
+        qs = self.qs
+        sA, sB, sC = self._scratch(A), self._scratch(B), self._scratch(C)
+        plan = qs.plan_contract(sC, sA, indA, sB, indB, indC, **kw, **opts)
+        qs.execute(plan, 1.0, 0.0)
+        torch.cuda.synchronize()
+        out = sC.parent.clone()
+        times = []
+        for _ in range(self.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            qs.execute(plan, 1.0, 0.0)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        plan.release()
+        if ref_store is not None and "ref" not in ref_store:
+            # the FP64 gather result on the same scratch data
+            ref_kw = dict(kw)
+            if A.dtype in (torch.float32, torch.complex64):
+                ref_kw["accumulator"] = "Float64"
+            rC = self._scratch(C)
+            rp = qs.plan_contract(rC, sA, indA, sB, indB, indC, method="native", **ref_kw)
+            qs.execute(rp, 1.0, 0.0)
+            torch.cuda.synchronize()
+            ref_store["ref"] = rC.parent.clone()
+            rp.release()
+        err = 0.0
+        if ref_store is not None:
+            ref = ref_store["ref"].to(torch.complex128 if out.is_complex() else torch.float64)
+            d = out.to(ref.dtype) - ref
+            nr = torch.linalg.vector_norm(ref).item()
+            err = torch.linalg.vector_norm(d).item() / nr if nr > 0 else torch.linalg.vector_norm(d).item()
+        return statistics.median(times), err
+
+    # ------------------------------------------------------------ API ---
+    def options(self, C, A, indA, B, indB, indC, **kw) -> dict:
+        """plan_contract keyword arguments for this contraction (tuned, or
+        from the cache)."""
+        qs = self.qs
+        hp = qs.plan_contract(C, A, indA, B, indB, indC, host_only=True, **kw)
+        if hp.path != "NestPath":
+            return {}
+        key = self.key(hp, C, A, B, kw.get("accumulator"), kw.get("conjA", False), kw.get("conjB", False))
+        hit = self.entries.get(key)
+        if hit is not None:
+            self.hits += 1
+            return dict(hit["options"])
+        self.misses += 1
+        target = 1e-13 if hp.compute_type in ("Float64", "ComplexF64") else 1e-5
+        ref_store = {}
+        results = []
+        for cand in self.candidates(hp):
+            opts = dict(cand)
+            while True:
+                if self._measure is not None:
+                    ms, err = self._measure(opts)
+                else:
+                    ms, err = self._run(opts, C, A, indA, B, indB, indC, kw, ref_store)
+                if err <= target or opts.get("method") != "ozaki" or opts.get("ozaki_slices", 6) >= 8:
+                    break
+                # raise the slice count from the default until the probe meets the target
+                opts = dict(opts, ozaki_slices=max(opts.get("ozaki_slices", 0), 6) + 1)
+            results.append({"options": opts, "ms": ms, "rel_err": err, "ok": err <= target})
+        ok = [r for r in results if r["ok"]] or results
+        best = min(ok, key=lambda r: r["ms"])
+        self.entries[key] = {"options": best["options"], "candidates": results, "target": target,
+                             "M": hp.m_length, "N": hp.n_length, "K": hp.k_length}
+        self.save()
+        return dict(best["options"])
+
+    def plan(self, C, A, indA, B, indB, indC, **kw):
+        return self.qs.plan_contract(C, A, indA, B, indB, indC, **kw, **self.options(C, A, indA, B, indB, indC, **kw))

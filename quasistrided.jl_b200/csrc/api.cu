@@ -289,6 +289,12 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
   } else {
     p->method = QS_METHOD_NATIVE;
   }
+  const int nt = p->opts.native_tile;
+  if (nt < 0 || nt > 3) {
+    delete p;
+    return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..3");
+  }
+  p->native_shape = (nt > 0 && !is_complex(p->T)) ? nt - 1 : direct_shape(p->T, p->N);
   if (!p->host_only) {
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) {
@@ -360,7 +366,7 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
     case QS_PATH_OUTER: e = launch_outer(p->T, op, alpha, beta, bcase, p->c_mfast, st); break;
     default:
       if (p->method == QS_METHOD_NATIVE) {
-        e = launch_direct(p->T, op, alpha, beta, bcase, p->a_mfast, p->b_nfast, st);
+        e = launch_direct(p->T, op, alpha, beta, bcase, p->a_mfast, p->b_nfast, p->native_shape, st);
       } else {
         int rc2 = tc_execute(p, alpha, beta, bcase, st, ev);
         if (rc2 == QS_OK && ev) ++p->prof_nexec;
@@ -491,6 +497,8 @@ int qs_plan_get_info(const qs_plan *p, qs_plan_info *info) {
   for (int d = 0; d < p->ng.D; ++d) info->n_labels[d] = p->ng.label[d];
   for (int d = 0; d < p->kg.D; ++d) info->k_labels[d] = p->kg.label[d];
   info->workspace_bytes = (int64_t)p->ws.bytes;
+  info->stride_class = (p->a_mfast ? 1 : 0) | (p->b_nfast ? 2 : 0) | (p->c_mfast ? 4 : 0);
+  info->native_tile = p->native_shape + 1;
   return QS_OK;
 }
 

@@ -381,10 +381,10 @@ static cudaError_t launch_direct_s(const Operands &op, const Scalars<T> &s, int 
 }
 
 template <class T>
-static cudaError_t launch_direct_t(int Tcode, const Operands &op, const double *alpha, const double *beta,
+static cudaError_t launch_direct_t(int shape, const Operands &op, const double *alpha, const double *beta,
                                    int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
   auto s = make_scalars<T>(alpha, beta, beta_case);
-  switch (direct_shape(Tcode, op.N)) {
+  switch (shape) {
     case 1: return launch_direct_s<T, 1>(op, s, a_mfast, b_nfast, st);
     case 2: return launch_direct_s<T, 2>(op, s, a_mfast, b_nfast, st);
     default: return launch_direct_s<T, 0>(op, s, a_mfast, b_nfast, st);
@@ -392,12 +392,12 @@ static cudaError_t launch_direct_t(int Tcode, const Operands &op, const double *
 }
 
 cudaError_t launch_direct(int T, const Operands &op, const double *alpha, const double *beta,
-                          int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
+                          int beta_case, int a_mfast, int b_nfast, int shape, cudaStream_t st) {
   switch (T) {
-    case QS_F32: return launch_direct_t<float>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    case QS_F64: return launch_direct_t<double>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    case QS_C32: return launch_direct_t<cplx<float>>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
-    default: return launch_direct_t<cplx<double>>(T, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_F32: return launch_direct_t<float>(shape, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_F64: return launch_direct_t<double>(shape, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    case QS_C32: return launch_direct_t<cplx<float>>(0, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
+    default: return launch_direct_t<cplx<double>>(0, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
   }
 }
 

@@ -115,7 +115,7 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
     if (acase == 0 || p->path != QS_PATH_NEST) {
       g->single.push_back(i);
     } else if (p->method == QS_METHOD_NATIVE) {
-      nat[3 * (p->T - QS_F32) + direct_shape(p->T, p->N)].push_back(i);
+      nat[3 * (p->T - QS_F32) + p->native_shape].push_back(i);
     } else {
       tcm[tc_group_class(p)].push_back(i);
     }

@@ -17,7 +17,7 @@ void count_launches(int n);
 cudaError_t launch_scale(int T, const Operands &op, const double *beta, int beta_case, int mfast,
                          cudaStream_t st);
 cudaError_t launch_direct(int T, const Operands &op, const double *alpha, const double *beta,
-                          int beta_case, int a_mfast, int b_nfast, cudaStream_t st);
+                          int beta_case, int a_mfast, int b_nfast, int shape, cudaStream_t st);
 cudaError_t launch_dot(int T, const Operands &op, const double *alpha, const double *beta,
                        int beta_case, cudaStream_t st);
 cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const double *beta,

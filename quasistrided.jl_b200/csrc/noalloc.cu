@@ -183,7 +183,7 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
   } else if (p.path == QS_PATH_OUTER) {
     e = launch_outer(p.T, op, alpha, beta, bcase, p.c_mfast, st);
   } else {
-    e = launch_direct(p.T, op, alpha, beta, bcase, p.a_mfast, p.b_nfast, st);
+    e = launch_direct(p.T, op, alpha, beta, bcase, p.a_mfast, p.b_nfast, direct_shape(p.T, p.N), st);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {

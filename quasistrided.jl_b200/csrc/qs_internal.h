@@ -113,6 +113,7 @@ struct qs_plan {
   int a_mfast = 0;  // A's M map is unit-stride (gather along M)
   int b_nfast = 0;  // B's N map is unit-stride (gather along N)
   int c_mfast = 0;  // C's M map is unit-stride
+  int native_shape = 0;  // gather-GEMM tile shape (direct_shape numbering)
   qs::TensorCoreGeom tc;
   qs::Workspace ws;
   // Instrumentation (qs_plan_profile): cudaEvent_t handles, kProfStages+1

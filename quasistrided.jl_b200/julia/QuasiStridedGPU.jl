@@ -39,6 +39,7 @@ Base.@kwdef struct QSPlanOptions
     ozaki_slices::Int32 = 0
     complex_mode::Int32 = 0
     flags::Int32 = 0
+    native_tile::Int32 = 0
 end
 
 const ELTYPE = Dict(Float32 => Int32(0), Float64 => Int32(1), ComplexF32 => Int32(2), ComplexF64 => Int32(3))
