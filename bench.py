@@ -491,6 +491,27 @@ def run_serving(args):
     print(json.dumps(result), flush=True)
 
 
+def init_ranks(world: int, backend: str = "nccl", timeout_s: int = 120) -> None:
+    """One process per GPU (torchrun sets RANK/WORLD_SIZE/MASTER_*); a short
+    process-group timeout so ranks that wait for each other fail instead of
+    hanging."""
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's value (the bench's whole-job time)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,9 +570,7 @@ def main():
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    init_ranks(world, "nccl")
     qs = load_engine()
     dev = torch.device("cuda", local)
 
@@ -609,11 +628,8 @@ def main():
             torch.cuda.synchronize()
     stage_ms, nexec = qs.stage_times(plan)
     qs.profile(plan, False)
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     value = world * FLOPS / (ms * 1e-3) / 1e12
 
@@ -640,11 +656,7 @@ def main():
         C_out.copy_(Cd, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, world, dev)
     e2e_value = world * FLOPS / (e2e_ms * 1e-3) / 1e12
 
     cpu = None
