@@ -491,6 +491,95 @@ def run_serving(args):
     print(json.dumps(result), flush=True)
 
 
+def run_mps(args):
+    """ComplexF64 MPS environment update as three pairwise contractions
+    (chi = 1024, D_W = 5, d = 2):
+        T1[w,al',s,be]   = L[al,w,al'] * A[al,s,be]                (5120 x 2048 x 1024)
+        T2[al',be,w',t]  = T1[w,al',s,be] * W[w,s,w',t]            (1048576 x 10 x 10)
+        out[be,w',be']   = T2[al',be,w',t] * conj(A)[al',t,be']    (5120 x 1024 x 2048)
+    One step = the three executes on reused plans.  Prints one JSON line."""
+    import torch
+    qs = load_engine()
+    from oracle import oracle as orc
+    chi, D, d = 1024, 5, 2
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20261203)
+
+    def crandn(*shape):
+        n = int(np.prod(shape))
+        return torch.randn(n, dtype=torch.complex128, device="cuda", generator=g)
+
+    L = crandn(chi, D, chi)
+    A = crandn(chi, d, chi)
+    W = crandn(D, d, D, d)
+    T1 = torch.zeros(D * chi * d * chi, dtype=torch.complex128, device="cuda")
+    T2 = torch.zeros(chi * chi * D * d, dtype=torch.complex128, device="cuda")
+    out = torch.zeros(chi * D * chi, dtype=torch.complex128, device="cuda")
+    V = lambda t, shape: qs.StridedView(t, shape, colmajor_strides(shape), 0)  # noqa: E731
+    Lv, Av, Wv = V(L, (chi, D, chi)), V(A, (chi, d, chi)), V(W, (D, d, D, d))
+    T1v, T2v, Ov = V(T1, (D, chi, d, chi)), V(T2, (chi, chi, D, d)), V(out, (chi, D, chi))
+    steps = [
+        ("T1=L*A", qs.plan_contract(T1v, Lv, (1, 2, 3), Av, (1, 4, 5), (2, 3, 4, 5)), 8.0 * 5120 * 2048 * 1024),
+        ("T2=T1*W", qs.plan_contract(T2v, T1v, (2, 3, 4, 5), Wv, (2, 4, 6, 7), (3, 5, 6, 7)), 8.0 * chi * chi * 10 * 10),
+        ("out=T2*conj(A)", qs.plan_contract(Ov, T2v, (3, 5, 6, 7), Av, (3, 7, 8), (5, 6, 8), conjB=True),
+         8.0 * 5120 * 1024 * 2048),
+    ]
+    total_flops = sum(f for _, _, f in steps)
+    for _ in range(args.warmup):
+        for _, p, _ in steps:
+            qs.execute(p, 1.0, 0.0)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    per = [0.0, 0.0, 0.0]
+    e_all0, e_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_all0.record()
+    for _ in range(args.steps):
+        evs[0].record()
+        for i, (_, p, _) in enumerate(steps):
+            qs.execute(p, 1.0, 0.0)
+            evs[i + 1].record()
+        torch.cuda.synchronize()
+        for i in range(3):
+            per[i] += evs[i].elapsed_time(evs[i + 1])
+    e_all1.record()
+    torch.cuda.synchronize()
+    per = [x / args.steps for x in per]
+    ms = sum(per)
+    # Accuracy per step on sampled outputs, each from the device's own inputs.
+    errs = []
+    host = lambda t: t.cpu().numpy()  # noqa: E731
+    samples = [
+        (host(T1), (D, chi, d, chi), host(L), (chi, D, chi), (1, 2, 3), host(A), (chi, d, chi), (1, 4, 5),
+         (2, 3, 4, 5), False),
+        (host(T2), (chi, chi, D, d), host(T1), (D, chi, d, chi), (2, 3, 4, 5), host(W), (D, d, D, d),
+         (2, 4, 6, 7), (3, 5, 6, 7), False),
+        (host(out), (chi, D, chi), host(T2), (chi, chi, D, d), (3, 5, 6, 7), host(A), (chi, d, chi), (3, 7, 8),
+         (5, 6, 8), True),
+    ]
+    nsamp = 4096
+    for got, sc, a, sa, ia, b, sb, ib, ic, cj in samples:
+        Ch = orc.HostView(np.zeros_like(got), sc, colmajor_strides(sc))
+        orc.brute(Ch, 1.0, orc.HostView(a, sa, colmajor_strides(sa)), ia, orc.HostView(b, sb, colmajor_strides(sb)),
+                  ib, 0.0, ic, conjB=cj, c_range=(0, nsamp))
+        ref = Ch.parent[:nsamp]
+        errs.append(float(np.linalg.norm(got[:nsamp] - ref) / np.linalg.norm(ref)))
+    bytes2 = (T1.numel() + W.numel() + T2.numel()) * 16
+    res = {
+        "metric": "contraction TFLOP/s (ComplexF64 MPS environment update, rel.err<=1e-13 vs FP64)",
+        "value": total_flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (ComplexF64)", "data": "synthetic (seeded complex N(0,1)/sqrt2)",
+        "config": {"workload": "mps_env_update_chi1024_DW5_d2", "flops": total_flops},
+        "stages": [{"step": name, "method": p.method, "complex_mode": p.complex_mode, "ms": t,
+                    "tflops": f / (t * 1e-3) / 1e12, "rel_err_sampled": e}
+                   for (name, p, f), t, e in zip(steps, per, errs)],
+        "step2_hbm_gbs": bytes2 / (per[1] * 1e-3) / 1e9,
+    }
+    print(json.dumps(res), flush=True)
+    for _, p, _ in steps:
+        p.release()
+
+
 def init_ranks(world: int, backend: str = "nccl", timeout_s: int = 120) -> None:
     """One process per GPU (torchrun sets RANK/WORLD_SIZE/MASTER_*); a short
     process-group timeout so ranks that wait for each other fail instead of
@@ -527,7 +616,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile", action="store_true",
                     help="profiling target: plan, one warm-up execute, --steps executes, exit")
-    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks", "serving"],
+    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks", "serving", "mps"],
                     help="blocks: 2000 uneven U(1) blocks, grouped vs graph vs plain launches")
     ap.add_argument("--blocks", type=int, default=2000)
     ap.add_argument("--modes", default="all",
@@ -565,6 +654,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "mps":
+        run_mps(args)
         return
 
     import torch

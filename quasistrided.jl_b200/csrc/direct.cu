@@ -220,6 +220,49 @@ __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJo
   direct_gemm_tile<T, Cfg>(op, s, j.a_mfast, j.b_nfast, lb % j.gx, lb / j.gx);
 }
 
+// ------------------------------------------------------------- skinny ----
+// N <= 16 and K <= 64 (the read-B-in-place case: B is tiny, C and A are
+// long): one thread per row of C, B and the K/N offset tables staged once per
+// CTA in shared memory, K ascending with fma (the ScalarKernel order, as in
+// the tiled kernel).  Bandwidth-bound: A is read once and C written once,
+// with no tile padding along N.
+constexpr int kSkinnyN = 16, kSkinnyK = 64;
+
+template <class T>
+__global__ void __launch_bounds__(256) skinny_kernel(Operands op, Scalars<T> s) {
+  __shared__ T Bs[kSkinnyK * kSkinnyN];
+  __shared__ int64_t sKA[kSkinnyK], sNC[kSkinnyN];
+  const int N = (int)op.N, K = (int)op.K;
+  for (int e = threadIdx.x; e < K * N; e += blockDim.x) {
+    const int k = e / N, j = e - k * N;
+    Bs[k * kSkinnyN + j] = Loader<T>::load(op.B, op.Bbase + op.offNB[j] + op.offKB[k], op.TB, op.conjB);
+  }
+  for (int k = threadIdx.x; k < K; k += blockDim.x) sKA[k] = op.offKA[k];
+  for (int j = threadIdx.x; j < N; j += blockDim.x) sNC[j] = op.offNC[j];
+  __syncthreads();
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < op.M;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    T acc[kSkinnyN];
+#pragma unroll
+    for (int j = 0; j < kSkinnyN; ++j) acc[j] = tzero<T>();
+    const int64_t am = op.Abase + op.offMA[m];
+    for (int k = 0; k < K; ++k) {
+      const T a = Loader<T>::load(op.A, am + sKA[k], op.TA, op.conjA);
+#pragma unroll
+      for (int j = 0; j < kSkinnyN; ++j)
+        if (j < N) acc[j] = cfma(a, Bs[k * kSkinnyN + j], acc[j]);
+    }
+    const int64_t cm = op.Cbase + op.offMC[m];
+#pragma unroll
+    for (int j = 0; j < kSkinnyN; ++j) {
+      if (j >= N) break;
+      const int64_t idx = cm + sNC[j];
+      const T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
+      store_c<T>(op.C, idx, op.TC, axpby(s, acc[j], old));
+    }
+  }
+}
+
 // ---------------------------------------------------------------- dot ----
 // out[q] = alpha * sum_k X[q,k] * v[k] + beta * C[q] for M == 1 or N == 1.
 // kmode = 1: one warp per output, lanes stride K (K unit-stride in X);
@@ -384,6 +427,11 @@ template <class T>
 static cudaError_t launch_direct_t(int shape, const Operands &op, const double *alpha, const double *beta,
                                    int beta_case, int a_mfast, int b_nfast, cudaStream_t st) {
   auto s = make_scalars<T>(alpha, beta, beta_case);
+  if (op.N <= kSkinnyN && op.K <= kSkinnyK) {
+    const int64_t blocks = (op.M + 255) / 256;
+    skinny_kernel<T><<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(op, s);
+    return cudaGetLastError();
+  }
   switch (shape) {
     case 1: return launch_direct_s<T, 1>(op, s, a_mfast, b_nfast, st);
     case 2: return launch_direct_s<T, 2>(op, s, a_mfast, b_nfast, st);

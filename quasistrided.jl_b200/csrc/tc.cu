@@ -1163,13 +1163,15 @@ int tc_auto_method(const qs_plan *p) {
   return is_double(p->T) ? QS_METHOD_OZAKI_I8 : QS_METHOD_BF16X3;
 }
 
-static int default_slices(int64_t K) {
-  // 6 base-254 digits (21 slice products) reach ~1e-14 relative Frobenius
-  // error at K = 2304 on uniform and 2^+-20-scaled inputs (7 signed 7-bit
-  // digits, 28 products, are needed for the same); longer K gets one more
-  // digit (the error grows like sqrt(K)).
+static int default_slices(int64_t K, bool cplx) {
+  // The relative error of s base-254 digits is about 254^-s times
+  // (row max / row rms of A + column max / column rms of B): ~1e-14 for
+  // s = 6 on uniform inputs at K = 2304 (max/rms = sqrt 3), but up to ~1e-13
+  // for Gaussian rows of a few thousand elements (max/rms ~ 4), which the
+  // 1m form of complex data (K doubled) reaches.  7 digits (28 products)
+  // for complex compute types and for K beyond 4096, else 6 (21 products).
   int s = 6;
-  if (K > 16384) s = 7;
+  if (cplx || K > 4096) s = 7;
   return s;
 }
 
@@ -1184,7 +1186,7 @@ void tc_geometry(qs_plan *p) {
   g.kmul = cx ? 2 : 1;
   const int64_t Mv = cx ? 2 * p->M : p->M, Kv = cx ? 2 * p->K : p->K;
   if (p->method == QS_METHOD_OZAKI_I8) {
-    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv);
+    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv, cx);
     p->ozaki_slices = g.nslices;
     g.kblocks = cdiv(Kv, 128);
     g.mtiles = cdiv(Mv, 128);

@@ -114,6 +114,23 @@ def test_native_narrow_n_tiles_bitwise(qs, orc, MKN, b_nfast):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("et", ["Float64", "ComplexF64", "Float32"])
+@pytest.mark.parametrize("MKN", [(70000, 10, 10), (5000, 64, 16), (3000, 7, 3)])
+def test_skinny_path(qs, orc, et, MKN):
+    # N <= 16, K <= 64: one thread per row, B in shared memory; the
+    # ScalarKernel FMA order, so real Float64 is bitwise equal to the oracle.
+    M, K, N = MKN
+    rng = np.random.default_rng(M + K + N)
+    A = colmajor_pair(qs, rng, (M, K), et)
+    B = colmajor_pair(qs, rng, (K, N), et)
+    C = colmajor_pair(qs, rng, (M, N), et)
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native")
+    if et == "Float64":
+        assert np.array_equal(got, ref)
+    else:
+        assert rel_fro(got, ref) <= 50 * K * eps(et)
+
+
 def test_permuted_zero_and_negative_strides_sliced_c(qs, orc):
     # test/execution/test_nest.jl:76-92
     rng = np.random.default_rng(11)
