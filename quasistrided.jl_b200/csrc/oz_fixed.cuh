@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(320, 1)
       named_bar_sync(1, 256);
       if (et < 128) {
         const int64_t n = n0 + et;
-        s_offN[et] = n < Pg.N ? Pg.offNC[n] : 0;
+        s_offN[et] = n < Pg.N ? c_col(Pg, n) : 0;
         s_expN[et] = n < Pg.N ? Pg.expB[n] : 0;
       }
       if constexpr (GROUPED) {
@@ -281,9 +281,9 @@ __global__ void __launch_bounds__(320, 1)
       const int64_t i = m0 + 32 * q + lane;
       const bool row_ok = i < P.M;
       const int eA = row_ok ? P.expA[i] : 0;
-      const int64_t crow = row_ok ? P.Cbase + P.offMC[P.cplx ? (i >> 1) : i] : 0;
+      const int64_t crow = row_ok ? P.Cbase + c_row(P, i) : 0;
       const bool row_store = row_ok && eA != kNonFinite;
-      if (row_store && (!P.cplx || (lane & 1) == 0)) prefetch_c_row(P, crow, s_offN, 64 * h, 64, n0);
+      if (row_store && (P.cplx != 1 || (lane & 1) == 0)) prefetch_c_row(P, crow, s_offN, 64 * h, 64, n0);
       bool first = true;
       if (!oz_drain_group<S, kG1>(P, accpar, first, sum, tbase, accf, acce, lane, abort)) break;
       if constexpr (NG > 1)

@@ -81,6 +81,8 @@ struct TensorCoreGeom {
   int64_t Mp = 0, Np = 0, Kp = 0;  // padded rows of A/B panels and K
   int64_t mtiles = 0, ntiles = 0, kblocks = 0;
   int rows_per_elem_a = 1;  // 1m: 2 real rows per complex row of A
+  int cols_per_elem_b = 1;  // planar: 2 real columns per complex column of B
+  int cplx_layout = 0;      // 0 real, 1 = 1m (A "1e", B "1r"), 2 = planar (A "1r", B "1e")
   int kmul = 1;             // 1m: 2 real K per complex K
   int nslices = 0;          // Ozaki slices (or 2 planes hi/lo for bf16x3)
   int64_t plane_bytes_a = 0, plane_bytes_b = 0;

@@ -62,10 +62,13 @@ struct PackArgs {
   int nslices;
   int32_t *exp_out;
   int32_t *flag_list, *flag_count;
-  // Complex operands as real matrices (the 1m method): 0 = real; 1 = "1e"
-  // (row 2i = [re, -im], row 2i+1 = [im, re] along K pairs; rows and K are
-  // doubled); 2 = "1r" (K pair = [re; im]; K doubled).  `rows`/`K` above are
-  // the real (virtual) extents; offR/offK index the complex elements.
+  // Complex operands as real matrices: 0 = real; 1 = "1e" (row 2i =
+  // [re, -im], row 2i+1 = [im, re] along K pairs; rows and K are doubled);
+  // 2 = "1r" (K pair = [re; im]; K doubled).  The 1m layout packs A as 1e
+  // and B as 1r; the planar layout A as 1r and B as 1e, so that a real row
+  // of C holds (re, im) of each complex element in adjacent columns.
+  // `rows`/`K` above are the real (virtual) extents; offR/offK index the
+  // complex elements.
   int cmode;
 };
 
@@ -285,7 +288,8 @@ struct GemmArgs {
   double alpha, beta;
   double alpha_im, beta_im;
   int beta_case;
-  int cplx;  // 1m: real rows 2i / 2i+1 are Re / Im of complex row i
+  int cplx;  // 0 real; 1 = 1m: real rows 2i / 2i+1 are Re / Im of complex
+             // row i; 2 = planar: real columns 2n / 2n+1 are Re / Im of n
   int *status;
   double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
 };
@@ -310,7 +314,37 @@ __device__ __forceinline__ void store_chunk_any(const GemmArgs &a, const R (&v)[
     idx = crow + s_offN[jj];
     return row_store && n0 + jj < a.N && finite;
   };
-  if (a.cplx) {
+  if (a.cplx == 2) {
+    // planar: columns 16c + 2u and 16c + 2u + 1 are Re and Im of one element
+    Scalars<cplx<R>> s;
+    s.alpha.re = (R)a.alpha; s.alpha.im = (R)a.alpha_im;
+    s.beta.re = (R)a.beta; s.beta.im = (R)a.beta_im;
+    s.beta_case = a.beta_case;
+#pragma unroll
+    for (int e0 = 0; e0 < 16; e0 += 2 * G) {
+      cplx<R> old[G];
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        R x;
+        int64_t idx;
+        const bool ok = prep(e0 + 2 * u, x, idx);
+        old[u] = (ok && a.beta_case != 0) ? load_c<cplx<R>>(a.C, idx, a.TC) : tzero<cplx<R>>();
+      }
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        R xr, xi;
+        int64_t idx, idx2;
+        const bool ok = prep(e0 + 2 * u, xr, idx);
+        prep(e0 + 2 * u + 1, xi, idx2);
+        if (ok) {
+          cplx<R> r;
+          r.re = xr;
+          r.im = xi;
+          store_c<cplx<R>>(a.C, idx, a.TC, axpby(s, r, old[u]));
+        }
+      }
+    }
+  } else if (a.cplx) {
     Scalars<cplx<R>> s;
     s.alpha.re = (R)a.alpha; s.alpha.im = (R)a.alpha_im;
     s.beta.re = (R)a.beta; s.beta.im = (R)a.beta_im;
@@ -447,6 +481,14 @@ constexpr size_t gemm_smem_bytes() {
   using Cfg = GemmCfg<KIND>;
   return 1024 + (size_t)Cfg::STAGES * (kTileM * kKBytes + Cfg::BN * kKBytes) + 1024 +
          Cfg::BN * (sizeof(int64_t) + sizeof(int32_t));
+}
+
+// C offsets of real (virtual) row i and real column n of the GEMM.
+__device__ __forceinline__ int64_t c_row(const GemmArgs &a, int64_t i) {
+  return a.offMC[a.cplx == 1 ? (i >> 1) : i];
+}
+__device__ __forceinline__ int64_t c_col(const GemmArgs &a, int64_t n) {
+  return a.offNC[a.cplx == 2 ? (n >> 1) : n];
 }
 
 // The problem table of a grouped launch: tile t of the launch belongs to
@@ -632,14 +674,14 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       named_bar_sync(1, 128);
       for (int j = et; j < BN; j += 128) {
         int64_t n = n0 + j;
-        s_offN[j] = n < P.N ? P.offNC[n] : 0;
+        s_offN[j] = n < P.N ? c_col(P, n) : 0;
         s_expN[j] = (KIND == KIND_I8 && n < P.N) ? P.expB[n] : 0;
       }
       named_bar_sync(1, 128);
       const int64_t i = m0 + 32 * q + lane;  // real (virtual) row
       const bool row_ok = i < P.M;
       const int eA = (KIND == KIND_I8 && row_ok) ? P.expA[i] : 0;
-      const int64_t crow = row_ok ? P.Cbase + P.offMC[P.cplx ? (i >> 1) : i] : 0;
+      const int64_t crow = row_ok ? P.Cbase + c_row(P, i) : 0;
       const bool row_store = row_ok && eA != kNonFinite;
       for (int g = 0; g < nseg; ++g, ++sc) {
         const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
@@ -899,14 +941,14 @@ __global__ void __launch_bounds__(320, 1)
       named_bar_sync(1, 256);
       if (et < 128) {
         const int64_t n = n0 + et;
-        s_offN[et] = n < a.N ? a.offNC[n] : 0;
+        s_offN[et] = n < a.N ? c_col(a, n) : 0;
         s_expN[et] = n < a.N ? a.expB[n] : 0;
       }
       named_bar_sync(1, 256);
       const int64_t i = m0 + 32 * q + lane;
       const bool row_ok = i < a.M;
       const int eA = row_ok ? a.expA[i] : 0;
-      const int64_t crow = row_ok ? a.Cbase + a.offMC[a.cplx ? (i >> 1) : i] : 0;
+      const int64_t crow = row_ok ? a.Cbase + c_row(a, i) : 0;
       const bool row_store = row_ok && eA != kNonFinite;
       bool first = true;
       for (int gi = 0; gi < sch.ngroups; ++gi) {
@@ -1085,11 +1127,12 @@ static OzSched build_oz_sched(int s) {
 // Non-finite rows of A / columns of B (flagged by the pack): those elements
 // of C are computed here directly in FP64 (IEEE semantics), and the GEMM's
 // epilogue skipped them.
-// T is double or cplx<double>.  The flagged row list holds real (virtual)
-// rows; for the 1m layout rows 2i and 2i+1 are both flagged and the even one
-// stands for complex row i.
+// T is double or cplx<double>.  The flagged lists hold real (virtual) rows
+// of the A and B panels: in the 1m layout (layout 1) rows 2i and 2i+1 of A
+// are both flagged and the even one stands for complex row i; in the planar
+// layout (2) the same holds for the rows of B (columns of C).
 template <class T>
-__device__ __forceinline__ void oz_fixup_range(const Operands &op, const Scalars<T> &s, int cplx,
+__device__ __forceinline__ void oz_fixup_range(const Operands &op, const Scalars<T> &s, int layout,
                                                const int32_t *rows, const int32_t *nrows,
                                                const int32_t *cols, const int32_t *ncols,
                                                const int32_t *expA, int64_t first, int64_t stride) {
@@ -1100,7 +1143,7 @@ __device__ __forceinline__ void oz_fixup_range(const Operands &op, const Scalars
     if (e < (int64_t)nr * op.N) {
       i = rows[e / op.N];
       j = e % op.N;
-      if (cplx) {
+      if (layout == 1) {
         if (i & 1) continue;
         i >>= 1;
       }
@@ -1108,7 +1151,11 @@ __device__ __forceinline__ void oz_fixup_range(const Operands &op, const Scalars
       int64_t f = e - (int64_t)nr * op.N;
       j = cols[f / op.M];
       i = f % op.M;
-      if (expA[cplx ? 2 * i : i] == kNonFinite) continue;  // done by the row pass
+      if (layout == 2) {
+        if (j & 1) continue;
+        j >>= 1;
+      }
+      if (expA[layout == 1 ? 2 * i : i] == kNonFinite) continue;  // done by the row pass
     }
     T acc = tzero<T>();
     for (int64_t k = 0; k < op.K; ++k) {
@@ -1136,7 +1183,7 @@ __device__ __forceinline__ void oz_fixup_job(const FixupJob &f, int64_t first, i
     s.alpha.re = f.alpha[0]; s.alpha.im = f.alpha[1];
     s.beta.re = f.beta[0]; s.beta.im = f.beta[1];
     s.beta_case = f.beta_case;
-    oz_fixup_range<cplx<double>>(f.op, s, 1, f.rows, f.nrows, f.cols, f.ncols, f.expA, first, stride);
+    oz_fixup_range<cplx<double>>(f.op, s, f.cplx, f.rows, f.nrows, f.cols, f.ncols, f.expA, first, stride);
   } else {
     Scalars<double> s;
     s.alpha = f.alpha[0];
@@ -1178,19 +1225,31 @@ static int default_slices(int64_t K, bool cplx) {
 void tc_geometry(qs_plan *p) {
   TensorCoreGeom &g = p->tc;
   g = TensorCoreGeom{};
-  // 1m: the real GEMM of a complex plan has 2M rows (A as "1e") and 2K
-  // columns of K (B as "1r").
+  // Complex plans run as one real GEMM with K doubled.  1m: A as "1e"
+  // (2M rows), B as "1r"; planar: A as "1r", B as "1e" (2N columns), so C's
+  // Re/Im sit in adjacent columns.  The expanded operand's panels are twice
+  // the other's, so by default the smaller side is expanded (planar when
+  // M > N); complex_mode forces one.
   const bool cx = is_complex(p->T);
-  p->complex_mode = cx ? QS_CPLX_1M : QS_CPLX_NONE;
-  g.rows_per_elem_a = cx ? 2 : 1;
+  int layout = 0;
+  if (cx) {
+    if (p->opts.complex_mode == QS_CPLX_PLANAR) layout = 2;
+    else if (p->opts.complex_mode == QS_CPLX_1M) layout = 1;
+    else layout = p->M > p->N ? 2 : 1;
+  }
+  g.cplx_layout = layout;
+  p->complex_mode = layout == 2 ? QS_CPLX_PLANAR : (layout == 1 ? QS_CPLX_1M : QS_CPLX_NONE);
+  g.rows_per_elem_a = layout == 1 ? 2 : 1;
+  g.cols_per_elem_b = layout == 2 ? 2 : 1;
   g.kmul = cx ? 2 : 1;
-  const int64_t Mv = cx ? 2 * p->M : p->M, Kv = cx ? 2 * p->K : p->K;
+  const int64_t Mv = p->M * g.rows_per_elem_a, Nv = p->N * g.cols_per_elem_b;
+  const int64_t Kv = cx ? 2 * p->K : p->K;
   if (p->method == QS_METHOD_OZAKI_I8) {
     g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv, cx);
     p->ozaki_slices = g.nslices;
     g.kblocks = cdiv(Kv, 128);
     g.mtiles = cdiv(Mv, 128);
-    g.ntiles = cdiv(p->N, 128);
+    g.ntiles = cdiv(Nv, 128);
     g.Mp = g.mtiles * 128;
     g.Np = g.ntiles * 128;
     g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
@@ -1203,7 +1262,7 @@ void tc_geometry(qs_plan *p) {
     g.nslices = 2;
     g.kblocks = cdiv(Kv, 64);
     g.mtiles = cdiv(Mv, 128);
-    g.ntiles = cdiv(p->N, 256);
+    g.ntiles = cdiv(Nv, 256);
     g.Mp = g.mtiles * 128;
     g.Np = g.ntiles * 256;
     g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
@@ -1237,7 +1296,7 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelB = q;
   if (p->method == QS_METHOD_OZAKI_I8) {
     // exponents (padded rows/cols), non-finite lists, their counters, status
-    size_t n = (size_t)(g.Mp + g.Np + g.Mp + p->N + 4);
+    size_t n = (size_t)(g.Mp + g.Np + g.Mp + g.Np + 4);
     if ((rc = tc_alloc(p, &q, n * sizeof(int32_t)))) return rc;
     int32_t *b = (int32_t *)q;
     p->ws.expA = b;
@@ -1291,15 +1350,16 @@ static PackArgs pack_args(const qs_plan *p, int side) {
     a.X = p->Adata; a.Xbase = p->Abase; a.TX = p->TA; a.conj = p->conjA;
     a.offR = p->ws.offM[0]; a.offK = p->ws.offK[0];
     a.rows = p->M * g.rows_per_elem_a; a.rows_pad = g.Mp; a.tile_rows = 128;
-    a.cmode = g.kmul == 2 ? 1 : 0;
+    a.cmode = g.cplx_layout == 1 ? 1 : (g.cplx_layout == 2 ? 2 : 0);
     a.rfast = p->a_mfast;
     a.panel = (uint8_t *)p->ws.panelA; a.plane = g.plane_bytes_a;
     a.exp_out = p->ws.expA;
   } else {
     a.X = p->Bdata; a.Xbase = p->Bbase; a.TX = p->TB; a.conj = p->conjB;
     a.offR = p->ws.offN[0]; a.offK = p->ws.offK[1];
-    a.rows = p->N; a.rows_pad = g.Np; a.tile_rows = p->method == QS_METHOD_BF16X3 ? 256 : 128;
-    a.cmode = g.kmul == 2 ? 2 : 0;
+    a.rows = p->N * g.cols_per_elem_b; a.rows_pad = g.Np;
+    a.tile_rows = p->method == QS_METHOD_BF16X3 ? 256 : 128;
+    a.cmode = g.cplx_layout == 1 ? 2 : (g.cplx_layout == 2 ? 1 : 0);
     a.rfast = p->b_nfast;
     a.panel = (uint8_t *)p->ws.panelB; a.plane = g.plane_bytes_b;
     a.exp_out = p->ws.expB;
@@ -1308,8 +1368,8 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
   if (p->method == QS_METHOD_OZAKI_I8) {
-    int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: N][2 counters]
-    int32_t *counters = lists + g.Mp + p->N;
+    int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
+    int32_t *counters = lists + g.Mp + g.Np;
     a.flag_list = side == 0 ? lists : lists + g.Mp;
     a.flag_count = counters + side;
   } else {
@@ -1342,8 +1402,8 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.offMC = p->ws.offM[1];
   a.offNC = p->ws.offN[1];
   a.M = p->M * g.rows_per_elem_a;
-  a.N = p->N;
-  a.cplx = g.kmul == 2;
+  a.N = p->N * g.cols_per_elem_b;
+  a.cplx = g.cplx_layout;
   a.alpha_im = alpha[1];
   a.beta_im = beta[1];
   a.alpha = alpha[0];
@@ -1370,9 +1430,9 @@ static FixupJob make_fixup_job(const qs_plan *p, const double *alpha, const doub
   f.alpha[0] = alpha[0]; f.alpha[1] = alpha[1];
   f.beta[0] = beta[0]; f.beta[1] = beta[1];
   f.beta_case = beta_case;
-  f.cplx = g.kmul == 2;
-  int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: N][2 counters]
-  int32_t *counters = lists + g.Mp + p->N;
+  f.cplx = g.cplx_layout;
+  int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
+  int32_t *counters = lists + g.Mp + g.Np;
   f.rows = lists;
   f.nrows = counters;
   f.cols = lists + g.Mp;
@@ -1388,7 +1448,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   int launches = 0;
   cudaError_t e;
   if (oz) {
-    int32_t *counters = p->ws.expA + g.Mp + g.Np + g.Mp + p->N;
+    int32_t *counters = p->ws.expA + g.Mp + g.Np + g.Mp + g.Np;
     e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
@@ -1564,7 +1624,7 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
       ZeroJob z;
       z.rowmax = (unsigned long long *)p->ws.rowmax;
       z.nwords = tg.Mp + tg.Np;
-      z.counters = p->ws.expA + tg.Mp + tg.Np + tg.Mp + p->N;
+      z.counters = p->ws.expA + tg.Mp + tg.Np + tg.Mp + tg.Np;
       zero.push_back(z);
       fix.push_back(make_fixup_job(p, al, be, bcase[g.idx[i]]));
     }

@@ -218,6 +218,56 @@ def test_complex_1m_ozaki(qs, orc, conj, beta):
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
 
 
+@pytest.mark.parametrize("mode", ["planar", None])
+@pytest.mark.parametrize("conj", [(False, False), (True, True), (False, True)])
+@pytest.mark.parametrize("beta", [0.0, 0.5 - 0.25j])
+def test_complex_planar_ozaki(qs, orc, mode, conj, beta):
+    # The planar layout (A as [re | im] along K, B expanded to 2N interleaved
+    # columns): C's Re/Im land in adjacent columns of one epilogue thread.
+    # M > N, so the default picks it too.
+    rng = np.random.default_rng(31)
+    M, K, N = 300, 150, 140
+    A = complex_pair(qs, rng, (M, K))
+    B = complex_pair(qs, rng, (K, N))
+    C = colmajor_pair(qs, rng, (M, N), "ComplexF64", fill=np.nan if beta == 0 else None)
+    got, ref, plan = run_pair(qs, orc, C, 1.25 + 0.5j, A, (1, 2), B, (2, 3), beta, (1, 3),
+                              conjA=conj[0], conjB=conj[1], precision=1, complex_mode=mode)
+    assert plan.method == "ozaki" and plan.complex_mode == "planar"
+    assert np.all(np.isfinite(got))
+    assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
+
+
+def test_complex_planar_nonfinite_and_f32(qs, orc):
+    rng = np.random.default_rng(32)
+    M, K, N = 260, 90, 140
+    A = complex_pair(qs, rng, (M, K))
+    b = (rng.standard_normal(K * N) + 1j * rng.standard_normal(K * N)) / np.sqrt(2)
+    b[K * 7 + 3] = complex(np.inf, 0)  # column 7 of B
+    B = Pair(qs, b, (K, N), (1, K))
+    C = colmajor_pair(qs, rng, (M, N), "ComplexF64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), precision=1,
+                              complex_mode="planar")
+    assert plan.complex_mode == "planar"
+    g = got.reshape(N, M).T
+    r = ref.reshape(N, M).T
+    assert np.array_equal(np.isnan(g), np.isnan(r)) and np.array_equal(np.isinf(g), np.isinf(r))
+    fin = np.isfinite(r)
+    assert rel_fro(g[fin], r[fin]) <= TOL64
+    # ComplexF32 through split BF16x3 in the planar layout
+    A32 = complex_pair(qs, rng, (M, K), "ComplexF32")
+    B32 = complex_pair(qs, rng, (K, N), "ComplexF32")
+    C32 = colmajor_pair(qs, rng, (M, N), "ComplexF32")
+    plan = qs.plan_contract(C32.dev, A32.dev, (1, 2), B32.dev, (2, 3), (1, 3), complex_mode="planar")
+    assert plan.method == "bf16x3" and plan.complex_mode == "planar"
+    qs.execute(plan, 0.5 + 1j, 0.25)
+    got = C32.device_parent().astype(np.complex128)
+    Ch = orc.HostView(C32.host.parent.astype(np.complex128), C32.host.size, C32.host.strides)
+    Ah = orc.HostView(A32.host.parent.astype(np.complex128), A32.host.size, A32.host.strides)
+    Bh = orc.HostView(B32.host.parent.astype(np.complex128), B32.host.size, B32.host.strides)
+    orc.brute(Ch, 0.5 + 1j, Ah, (1, 2), Bh, (2, 3), 0.25, (1, 3))
+    assert rel_fro(got, Ch.parent) <= TOL32, rel_fro(got, Ch.parent)
+
+
 def test_complex_mps_environment_steps(qs, orc):
     # The MPS environment update at chi = 64: T1 = L*A, T2 = T1*W,
     # out = T2*conj(A) (the last step conjugates on load).
