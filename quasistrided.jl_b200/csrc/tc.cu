@@ -223,10 +223,17 @@ __device__ __forceinline__ void oz_slice_block(const PackArgs &a, const unsigned
     uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
-      const double y = x[kk] * 254.0;
-      const double d = rint(y);
-      x[kk] = y - d;
-      const uint32_t byte = (uint32_t)((int32_t)d) & 0xFFu;
+      // y = 254 x; d = y rounded to the nearest integer (ties to even, like
+      // rint) by adding and removing 1.5 * 2^52, whose low word then holds
+      // d in two's complement; x = y - d.  Four full-rate FP64 adds and
+      // multiplies, no rounding or conversion instructions; the _rn
+      // intrinsics keep the compiler from fusing the steps.
+      constexpr double kRound = 6755399441055744.0;
+      const double y = __dmul_rn(x[kk], 254.0);
+      const double t = __dadd_rn(y, kRound);
+      const double d = __dsub_rn(t, kRound);
+      x[kk] = __dsub_rn(y, d);
+      const uint32_t byte = (uint32_t)__double2loint(t) & 0xFFu;
       w[kk >> 2] |= byte << (8 * (kk & 3));
     }
     *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
