@@ -1209,11 +1209,15 @@ __global__ void __launch_bounds__(256) oz_fixup_kernel(const __grid_constant__ F
 static int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 int tc_auto_method(const qs_plan *p) {
-  // The tensor-core paths pay a pack pass and pad to 128-row tiles: worth it
-  // once every extent fills a tile.  Complex plans run the 1m formulation,
-  // whose real GEMM has 2M rows and 2K columns.
-  const int64_t mr = is_complex(p->T) ? 2 * p->M : p->M;
-  if (mr < 128 || p->N < 128 || p->K < 64) return QS_METHOD_NATIVE;
+  // The tensor-core paths pay a pack pass, five more launches and pad to
+  // 128 x 128 tiles: worth it once M fills a tile, N at least half of one,
+  // K one K block, and the work is past the point where launch latency
+  // dominates (M*N*K >= 2^26).  Complex plans count their real GEMM
+  // (2 real rows or columns per complex one).
+  const int64_t m = is_complex(p->T) ? 2 * p->M : p->M;
+  const int64_t n = is_complex(p->T) ? 2 * p->N : p->N;
+  if (m < 128 || n < 64 || p->K < 64) return QS_METHOD_NATIVE;
+  if ((double)p->M * (double)p->N * (double)p->K < 67108864.0) return QS_METHOD_NATIVE;
   return is_double(p->T) ? QS_METHOD_OZAKI_I8 : QS_METHOD_BF16X3;
 }
 
