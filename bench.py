@@ -580,6 +580,79 @@ def run_mps(args):
         p.release()
 
 
+def run_matmul(args):
+    """The permuted matmul C[a,n,b] = sum_k A[a,k,b] * B[k,n] (a=96, k=128,
+    b=32, n=80; alpha = 1, beta = 0; M = (a,b) is not contiguous in C), in
+    Float64: microseconds per call for execute on a reused plan, the same
+    replayed as a CUDA graph, and one-shot contract (plan, execute, release).
+    Launch-latency bound (63 MFLOP).  Prints one JSON line."""
+    import torch
+    qs = load_engine()
+    from oracle import oracle as orc
+    a, k, b, n = 96, 128, 32, 80
+    rng = np.random.default_rng(20261203)
+    A_h = rng.standard_normal(a * k * b)
+    B_h = rng.standard_normal(k * n)
+    sa, sb, sc = (a, k, b), (k, n), (a, n, b)
+    Ad, Bd = torch.from_numpy(A_h).cuda(), torch.from_numpy(B_h).cuda()
+    Cd = torch.zeros(a * n * b, dtype=torch.float64, device="cuda")
+    Av = qs.StridedView(Ad, sa, colmajor_strides(sa), 0)
+    Bv = qs.StridedView(Bd, sb, colmajor_strides(sb), 0)
+    Cv = qs.StridedView(Cd, sc, colmajor_strides(sc), 0)
+    labels = ((1, 2, 3), (2, 4), (1, 4, 3))
+    flops = 2.0 * a * b * n * k
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return 1e3 * e0.elapsed_time(e1) / steps, 1e6 * (time.perf_counter() - t0) / steps
+
+    plan = qs.plan_contract(Cv, Av, labels[0], Bv, labels[1], labels[2])
+    gplan = qs.plan_contract(Cv, Av, labels[0], Bv, labels[1], labels[2], cuda_graph=True)
+    steps = max(args.steps, 200)
+    res = {}
+    res["execute_us"], res["execute_host_us"] = timed(lambda: qs.execute(plan, 1.0, 0.0), steps)
+    res["graph_us"], res["graph_host_us"] = timed(lambda: qs.execute(gplan, 1.0, 0.0), steps)
+    res["contract_us"], res["contract_host_us"] = timed(
+        lambda: qs.contract(Cv, 1.0, Av, labels[0], Bv, labels[1], 0.0, labels[2]), max(args.steps, 50))
+    qs.execute(plan, 1.0, 0.0)
+    torch.cuda.synchronize()
+    got = Cd.cpu().numpy()
+    Ch = orc.HostView(np.zeros(a * n * b), sc, colmajor_strides(sc))
+    orc.brute(Ch, 1.0, orc.HostView(A_h, sa, colmajor_strides(sa)), labels[0],
+              orc.HostView(B_h, sb, colmajor_strides(sb)), labels[1], 0.0, labels[2],
+              korder=list(plan.k_labels))
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 2.0:
+        Cn = orc.HostView(np.zeros(a * n * b), sc, colmajor_strides(sc))
+        orc.nest_f64(Cn, 1.0, orc.HostView(A_h, sa, colmajor_strides(sa)), labels[0],
+                     orc.HostView(B_h, sb, colmajor_strides(sb)), labels[1], 0.0, labels[2], threads=1)
+        reps += 1
+    cpu_us = 1e6 * (time.perf_counter() - t0) / reps
+    print(json.dumps({
+        "metric": "permuted matmul latency (Float64, us per execute on a reused plan)",
+        "value": res["execute_us"], "unit": "us", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1))",
+        "config": {"workload": "matmul_a96_k128_b32_n80", "method": plan.method, "flops": flops},
+        "tflops": flops / (res["execute_us"] * 1e-6) / 1e12, "modes_us": res,
+        "bitwise_equal_to_oracle": bool(np.array_equal(got, Ch.parent)),
+        "cpu_baseline": {"value": cpu_us, "unit": "us", "cores": 1, "kind": "port",
+                         "sample": f"{reps} full runs of the oracle's nest restatement, 1 thread"},
+    }), flush=True)
+    plan.release()
+    gplan.release()
+
+
 def init_ranks(world: int, backend: str = "nccl", timeout_s: int = 120) -> None:
     """One process per GPU (torchrun sets RANK/WORLD_SIZE/MASTER_*); a short
     process-group timeout so ranks that wait for each other fail instead of
@@ -616,7 +689,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile", action="store_true",
                     help="profiling target: plan, one warm-up execute, --steps executes, exit")
-    ap.add_argument("--workload", default="permuted4", choices=["permuted4", "blocks", "serving", "mps"],
+    ap.add_argument("--workload", default="permuted4",
+                    choices=["permuted4", "blocks", "serving", "mps", "matmul"],
                     help="blocks: 2000 uneven U(1) blocks, grouped vs graph vs plain launches")
     ap.add_argument("--blocks", type=int, default=2000)
     ap.add_argument("--modes", default="all",
@@ -657,6 +731,9 @@ def main():
         return
     if args.workload == "mps":
         run_mps(args)
+        return
+    if args.workload == "matmul":
+        run_matmul(args)
         return
 
     import torch
