@@ -129,8 +129,9 @@ typedef struct qs_plan_options {
   int32_t ozaki_slices;    /* 0 = chosen from K for 1e-13; else 2..10 */
   int32_t complex_mode;    /* QS_CPLX_*; 0 = default for the method */
   int32_t flags;           /* QS_PLAN_* */
-  int32_t native_tile;     /* gather-GEMM tile: 0 = by N; 1 = 64x64, 2 = 128x32,
-                              3 = 256x16 (real compute types; the autotuner's knob) */
+  int32_t native_tile;     /* gather-GEMM tile: 0 = by M and N; 1 = 64x64, 2 = 128x32,
+                              3 = 256x16, 4 = 32x32 (real compute types; the
+                              autotuner's knob) */
 } qs_plan_options;
 
 typedef struct qs_plan_info {
@@ -149,7 +150,7 @@ typedef struct qs_plan_info {
   int64_t workspace_bytes;
   int32_t stride_class;  /* bit 0: A's M map unit-stride, bit 1: B's N map,
                             bit 2: C's M map (the autotuner's stride class) */
-  int32_t native_tile;   /* gather-GEMM tile in use (1..3 as in the options) */
+  int32_t native_tile;   /* gather-GEMM tile in use (1..4 as in the options) */
 } qs_plan_info;
 
 typedef struct qs_plan qs_plan;

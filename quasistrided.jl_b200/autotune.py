@@ -6,7 +6,7 @@ while meeting the accuracy target:
 * method: the gather GEMM (``native``) or the tensor-core path (``ozaki`` for
   Float64/ComplexF64, ``bf16x3`` for Float32/ComplexF32);
 * the Ozaki GEMM kernel (grouped diagonals, or one product per stage);
-* the gather GEMM's tile shape (64x64, 128x32, 256x16; real types);
+* the gather GEMM's tile shape (64x64, 128x32, 256x16, 32x32; real types);
 * the Ozaki slice count: the default for K, raised while a probe on random
   data of the problem's layout misses the target (relative Frobenius error
   against the FP64 gather result: 1e-13 for Float64, 1e-5 for Float32).
@@ -98,7 +98,7 @@ class Autotuner:
         dbl = hp.compute_type in ("Float64", "ComplexF64")
         out = []
         if real:
-            out += [{"method": "native", "native_tile": t} for t in (1, 2, 3)]
+            out += [{"method": "native", "native_tile": t} for t in (1, 2, 3, 4)]
         else:
             out.append({"method": "native"})
         if dbl:

@@ -182,8 +182,18 @@ template <class T>
 struct DirectShape<T, 1, false> { using Cfg = DirectCfg<T, 128, 32, 16, 4>; };
 template <class T>
 struct DirectShape<T, 2, false> { using Cfg = DirectCfg<T, 256, 16, 8, 4>; };
+template <class T>
+struct DirectShape<T, 3, false> { using Cfg = DirectCfg<T, 32, 32, 16, 2>; };
 template <class T, int SHAPE>
 struct DirectShape<T, SHAPE, true> { using Cfg = DirectCfg<T, 32, 32, 16, 2>; };
+
+// Plans: a small problem whose 64 x 64 grid would not fill the GPU takes
+// 32 x 32 tiles (four times the CTAs).
+int direct_shape_mn(int T, int64_t M, int64_t N) {
+  int s = direct_shape(T, N);
+  if (s == 0 && T != QS_C32 && T != QS_C64 && ((M + 63) / 64) * ((N + 63) / 64) < 148) s = 3;
+  return s;
+}
 
 int direct_shape(int T, int64_t N) {
   if (T == QS_C32 || T == QS_C64) return 0;
@@ -435,6 +445,7 @@ static cudaError_t launch_direct_t(int shape, const Operands &op, const double *
   switch (shape) {
     case 1: return launch_direct_s<T, 1>(op, s, a_mfast, b_nfast, st);
     case 2: return launch_direct_s<T, 2>(op, s, a_mfast, b_nfast, st);
+    case 3: return launch_direct_s<T, 3>(op, s, a_mfast, b_nfast, st);
     default: return launch_direct_s<T, 0>(op, s, a_mfast, b_nfast, st);
   }
 }
@@ -522,6 +533,7 @@ static int native_group_build_t(NativeGroup &g, const Operands *ops, const doubl
     if (is_complex(g.T)) bm = bn = 32;
     else if (g.shape == 1) bm = 128, bn = 32;
     else if (g.shape == 2) bm = 256, bn = 16;
+    else if (g.shape == 3) bm = 32, bn = 32;
     const int64_t gx = (j.op.M + bm - 1) / bm, gy = (j.op.N + bn - 1) / bn;
     if (gx > INT32_MAX || blocks + gx * gy > INT32_MAX) return fail(QS_EINVAL, "ArgumentError: grouped launch too large");
     j.gx = (int)gx;
@@ -555,6 +567,7 @@ static cudaError_t native_group_launch_t(const NativeGroup &g, cudaStream_t st) 
   switch (g.shape) {
     case 1: native_group_launch_s<T, 1>(g, st); break;
     case 2: native_group_launch_s<T, 2>(g, st); break;
+    case 3: native_group_launch_s<T, 3>(g, st); break;
     default: native_group_launch_s<T, 0>(g, st); break;
   }
   return cudaGetLastError();

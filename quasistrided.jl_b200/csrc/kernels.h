@@ -26,7 +26,7 @@ cudaError_t launch_outer(int T, const Operands &op, const double *alpha, const d
 // Native (gather) GEMMs of many plans of one compute type as one launch.
 struct NativeGroup {
   int T = 0;
-  int shape = 0;                 // direct_shape(T, N) of every member
+  int shape = 0;                 // tile shape (direct_shape_mn numbering) of every member
   std::vector<qs_plan *> plans;  // K-descending
   std::vector<int> idx;          // position of each plan in the group's alpha/beta arrays
   std::vector<uint8_t> image;    // host image of the job table
@@ -43,6 +43,9 @@ cudaError_t native_group_launch(const NativeGroup &g, cudaStream_t st);
 // Tile shape of the gather GEMM for compute type T and N (0: 64x64,
 // 1: 128x32, 2: 256x16; complex: 0 = 32x32).
 int direct_shape(int T, int64_t N);
+// The plan's choice: direct_shape, or 3 (32x32) when a 64x64 grid would not
+// fill the GPU.
+int direct_shape_mn(int T, int64_t M, int64_t N);
 
 // The operands of a plan as the kernels read them.
 Operands make_operands(const qs_plan *p);

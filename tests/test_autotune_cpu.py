@@ -35,6 +35,7 @@ def fake(times, errs=None, calls=None):
 
 
 T64 = {("native", 1, False): 5.0, ("native", 2, False): 4.0, ("native", 3, False): 6.0,
+       ("native", 4, False): 7.0,
        ("ozaki", 0, False): 1.0, ("ozaki", 0, True): 1.5}
 
 
@@ -45,11 +46,11 @@ def test_picks_fastest_and_caches_on_disk(qs, at, tmp_path):
     C, A, ia, B, ib, ic = views(qs, 300, 200, 260)
     opts = t.options(C, A, ia, B, ib, ic)
     assert opts == {"method": "ozaki"}
-    assert len(calls) == 5 and t.misses == 1
+    assert len(calls) == 6 and t.misses == 1
     # same class (sizes in the same log2 buckets): a hit, no measurement
     C2, A2, _, B2, _, _ = views(qs, 400, 250, 300)
     assert t.options(C2, A2, ia, B2, ib, ic) == {"method": "ozaki"}
-    assert t.hits == 1 and len(calls) == 5
+    assert t.hits == 1 and len(calls) == 6
     # a new process reads the file
     t2 = at.Autotuner(qs, path=path, measure=fake(T64, calls=calls), device_name="B200")
     assert t2.options(C, A, ia, B, ib, ic) == {"method": "ozaki"} and t2.hits == 1
@@ -81,6 +82,7 @@ def test_slices_raised_until_accurate(qs, at, tmp_path):
 
 def test_float32_candidates_and_non_nest(qs, at, tmp_path):
     T32 = {("native", 1, False): 3.0, ("native", 2, False): 2.0, ("native", 3, False): 2.5,
+           ("native", 4, False): 2.6,
            ("bf16x3", 0, False): 2.2}
     t = at.Autotuner(qs, path=str(tmp_path / "f.json"), measure=fake(T32), device_name="B200")
     C, A, ia, B, ib, ic = views(qs, 300, 200, 20, dtype=torch.float32)

@@ -37,7 +37,7 @@ def test_tuned_plan_matches_oracle_and_is_cached(qs, orc, tmp_path, et, MKN, tol
     assert t2.options(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3)) == opts and t2.hits == 1
 
 
-@pytest.mark.parametrize("tile", [1, 2, 3])
+@pytest.mark.parametrize("tile", [1, 2, 3, 4])
 def test_native_tile_override_bitwise(qs, orc, tile):
     rng = np.random.default_rng(tile)
     M, K, N = 333, 97, 45

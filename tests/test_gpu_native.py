@@ -131,6 +131,19 @@ def test_skinny_path(qs, orc, et, MKN):
         assert rel_fro(got, ref) <= 50 * K * eps(et)
 
 
+def test_small_problem_32x32_tiles_bitwise(qs, orc):
+    # The c0 permuted matmul (M = (a,b) = 96*32, N = 80, K = 128): a 64x64
+    # grid would leave SMs idle, so the plan takes 32x32 tiles; same FMA
+    # order, so bitwise equal to the oracle.
+    rng = np.random.default_rng(96)
+    A = colmajor_pair(qs, rng, (96, 128, 32), "Float64")
+    B = colmajor_pair(qs, rng, (128, 80), "Float64")
+    C = colmajor_pair(qs, rng, (96, 80, 32), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2, 3), B, (2, 4), 0.0, (1, 4, 3))
+    assert plan.method == "native" and plan.native_tile == 4
+    assert np.array_equal(got, ref)
+
+
 def test_permuted_zero_and_negative_strides_sliced_c(qs, orc):
     # test/execution/test_nest.jl:76-92
     rng = np.random.default_rng(11)

@@ -43,9 +43,9 @@ def make_requests(sv, rng):
     # (shapeA, indA, shapeB, indB, indC, dtype, beta)
     cases = [
         ((96, 128, 32), (1, 2, 3), (128, 80), (2, 4), (1, 4, 3), np.float64, 0.0),       # permuted matmul, gather
-        ((256, 192), (1, 2), (192, 300), (2, 3), (1, 3), np.float64, 0.5),                # Ozaki
-        ((200, 130), (1, 2), (130, 260), (2, 3), (3, 1), np.float32, 0.0),                # BF16x3, C transposed
-        ((128, 96), (1, 2), (96, 140), (2, 3), (1, 3), np.complex128, 0.5),               # Ozaki 1m
+        ((512, 384), (1, 2), (384, 400), (2, 3), (1, 3), np.float64, 0.5),                # Ozaki
+        ((512, 256), (1, 2), (256, 600), (2, 3), (3, 1), np.float32, 0.0),                # BF16x3, C transposed
+        ((400, 300), (1, 2), (300, 600), (2, 3), (1, 3), np.complex128, 0.5),             # Ozaki, complex
         ((12, 9, 7), (1, 2, 3), (7, 9, 11), (3, 2, 4), (4, 1), np.float32, 0.0),          # gather, 2 K labels
         ((30, 20, 10), (3, 1, 2), (10, 40), (2, 4), (1, 4, 3), np.complex128, 0.0),       # gather complex
         ((64, 64), (1, 2), (64, 1), (2, 3), (1, 3), np.float64, 0.0),                     # dot path
@@ -81,7 +81,7 @@ def run(qs, sv, reqs, residents, budget, max_tick_requests=512):
     return srv
 
 
-@pytest.mark.parametrize("budget", [8 << 30, 12 << 20])
+@pytest.mark.parametrize("budget", [8 << 30, 24 << 20])
 def test_alone_equals_in_mix(qs, orc, budget):
     sv, _ = modules(qs)
     rng = np.random.default_rng(42)
@@ -95,7 +95,7 @@ def test_alone_equals_in_mix(qs, orc, budget):
         run(qs, sv, [alone], residents, 8 << 30)
         assert m.error is None and alone.error is None
         assert np.array_equal(m.result, alone.result), r.indC
-    # oracle on every request (binary128 for the tensor-core ones)
+    # FP64 oracle on every request (its own error is far below the bounds)
     for r, m in zip(reqs, mix):
         A = residents[r.A] if isinstance(r.A, str) else r.A
         dt = np.dtype(r.dtype)
@@ -103,8 +103,7 @@ def test_alone_equals_in_mix(qs, orc, budget):
         C = HostView((r.C0.copy() if r.C0 is not None else np.zeros(Cshape, dtype=dt)).ravel(order="F"),
                      Cshape, col_strides(Cshape))
         orc.brute(C, r.alpha, HostView(A.ravel(order="F"), A.shape, col_strides(A.shape)), r.indA,
-                  HostView(r.B.ravel(order="F"), r.B.shape, col_strides(r.B.shape)), r.indB, r.beta, r.indC,
-                  precision=1)
+                  HostView(r.B.ravel(order="F"), r.B.shape, col_strides(r.B.shape)), r.indB, r.beta, r.indC)
         ref = C.parent
         got = m.result.ravel(order="F")
         tol = 1e-5 if dt in (np.float32, np.complex64) else 1e-13

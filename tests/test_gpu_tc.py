@@ -47,11 +47,17 @@ def test_ozaki_matmul_matches_oracle(qs, orc, MKN, beta, per_product):
 
 
 def test_ozaki_is_the_default_for_float64(qs):
+    # Past M*N*K = 2^26 the default is the Ozaki path; below it (and for
+    # N < 64) the single-launch gather kernel.
     rng = np.random.default_rng(0)
-    A = uniform_pair(qs, rng, (256, 256))
-    B = uniform_pair(qs, rng, (256, 256))
-    C = colmajor_pair(qs, rng, (256, 256), "Float64")
+    A = uniform_pair(qs, rng, (512, 512))
+    B = uniform_pair(qs, rng, (512, 512))
+    C = colmajor_pair(qs, rng, (512, 512), "Float64")
     assert qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3)).method == "ozaki"
+    A2 = uniform_pair(qs, rng, (300, 200))
+    B2 = uniform_pair(qs, rng, (200, 260))
+    C2 = colmajor_pair(qs, rng, (300, 260), "Float64")
+    assert qs.plan_contract(C2.dev, A2.dev, (1, 2), B2.dev, (2, 3), (1, 3)).method == "native"
 
 
 @pytest.mark.parametrize("wide", [False, True])
@@ -151,7 +157,7 @@ def test_ozaki_mixed_input_eltypes(qs, orc):
     A = uniform_pair(qs, rng, (300, 200), et="Float32")
     B = uniform_pair(qs, rng, (200, 260))
     C = colmajor_pair(qs, rng, (300, 260), "Float64")
-    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1)
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1, method="ozaki")
     assert plan.method == "ozaki"
     assert rel_fro(got, ref) <= TOL64
 
@@ -163,7 +169,7 @@ def test_bf16x3_float32_matches_oracle(qs, orc, MKN):
     A = uniform_pair(qs, rng, (M, K), et="Float32")
     B = uniform_pair(qs, rng, (K, N), et="Float32")
     C = colmajor_pair(qs, rng, (M, N), "Float32")
-    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3))
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3), method="bf16x3")
     assert plan.method == "bf16x3"
     qs.execute(plan, 1.5, 0.5)
     got = C.device_parent()
@@ -212,7 +218,7 @@ def test_complex_1m_ozaki(qs, orc, conj, beta):
     B = complex_pair(qs, rng, (K, N))
     C = colmajor_pair(qs, rng, (M, N), "ComplexF64", fill=np.nan if beta == 0 else None)
     got, ref, plan = run_pair(qs, orc, C, 1.25 + 0.5j, A, (1, 2), B, (2, 3), beta, (1, 3),
-                              conjA=conj[0], conjB=conj[1], precision=1)
+                              conjA=conj[0], conjB=conj[1], precision=1, method="ozaki")
     assert plan.method == "ozaki" and plan.complex_mode == "1m"
     assert np.all(np.isfinite(got))
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
@@ -231,7 +237,7 @@ def test_complex_planar_ozaki(qs, orc, mode, conj, beta):
     B = complex_pair(qs, rng, (K, N))
     C = colmajor_pair(qs, rng, (M, N), "ComplexF64", fill=np.nan if beta == 0 else None)
     got, ref, plan = run_pair(qs, orc, C, 1.25 + 0.5j, A, (1, 2), B, (2, 3), beta, (1, 3),
-                              conjA=conj[0], conjB=conj[1], precision=1, complex_mode=mode)
+                              conjA=conj[0], conjB=conj[1], precision=1, complex_mode=mode, method="ozaki")
     assert plan.method == "ozaki" and plan.complex_mode == "planar"
     assert np.all(np.isfinite(got))
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
@@ -246,7 +252,7 @@ def test_complex_planar_nonfinite_and_f32(qs, orc):
     B = Pair(qs, b, (K, N), (1, K))
     C = colmajor_pair(qs, rng, (M, N), "ComplexF64")
     got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 0.5, (1, 3), precision=1,
-                              complex_mode="planar")
+                              complex_mode="planar", method="ozaki")
     assert plan.complex_mode == "planar"
     g = got.reshape(N, M).T
     r = ref.reshape(N, M).T
@@ -257,7 +263,8 @@ def test_complex_planar_nonfinite_and_f32(qs, orc):
     A32 = complex_pair(qs, rng, (M, K), "ComplexF32")
     B32 = complex_pair(qs, rng, (K, N), "ComplexF32")
     C32 = colmajor_pair(qs, rng, (M, N), "ComplexF32")
-    plan = qs.plan_contract(C32.dev, A32.dev, (1, 2), B32.dev, (2, 3), (1, 3), complex_mode="planar")
+    plan = qs.plan_contract(C32.dev, A32.dev, (1, 2), B32.dev, (2, 3), (1, 3), complex_mode="planar",
+                            method="bf16x3")
     assert plan.method == "bf16x3" and plan.complex_mode == "planar"
     qs.execute(plan, 0.5 + 1j, 0.25)
     got = C32.device_parent().astype(np.complex128)
@@ -278,7 +285,8 @@ def test_complex_mps_environment_steps(qs, orc):
     W = complex_pair(qs, rng, (D, d, D, d))
     # labels: al=1, w=2, al'=3, s=4, be=5, w'=6, t=7, be'=8
     T1 = colmajor_pair(qs, rng, (D, chi, d, chi), "ComplexF64", fill=0)
-    got, ref, p1 = run_pair(qs, orc, T1, 1, L, (1, 2, 3), A, (1, 4, 5), 0, (2, 3, 4, 5), precision=1)
+    got, ref, p1 = run_pair(qs, orc, T1, 1, L, (1, 2, 3), A, (1, 4, 5), 0, (2, 3, 4, 5), precision=1,
+                            method="ozaki")
     assert p1.method == "ozaki" and rel_fro(got, ref) <= TOL64
     T1.host.parent[:] = got  # continue from the device result on both sides
     T2 = colmajor_pair(qs, rng, (chi, chi, D, d), "ComplexF64", fill=0)
@@ -299,7 +307,7 @@ def test_complex_times_real_and_nonfinite(qs, orc):
     b[5] = np.nan  # column 0 of B
     B = Pair(qs, b, (K, N), (1, K))
     C = colmajor_pair(qs, rng, (M, N), "ComplexF64")
-    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1)
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2), B, (2, 3), 1.0, (1, 3), precision=1, method="ozaki")
     assert plan.method == "ozaki"
     g = got.reshape(N, M).T
     r = ref.reshape(N, M).T
@@ -314,7 +322,7 @@ def test_complex_f32_bf16x3(qs, orc):
     A = complex_pair(qs, rng, (M, K), "ComplexF32")
     B = complex_pair(qs, rng, (K, N), "ComplexF32")
     C = colmajor_pair(qs, rng, (M, N), "ComplexF32")
-    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3), conjA=True)
+    plan = qs.plan_contract(C.dev, A.dev, (1, 2), B.dev, (2, 3), (1, 3), conjA=True, method="bf16x3")
     assert plan.method == "bf16x3" and plan.complex_mode == "1m"
     qs.execute(plan, 0.5 + 1j, 0.25)
     got = C.device_parent().astype(np.complex128)
