@@ -11,6 +11,11 @@ explicit flush runs between steps.
 Prints one JSON line (rank 0).  ``--impl reference`` times the CPU arm: the
 oracle's restatement of the reference's five-loop nest (QuasiStrided.jl is
 Julia and cannot run here) on the host cores.
+
+Other workloads (``--workload``): ``matmul`` (the permuted matmul, latency),
+``mps`` (ComplexF64 MPS environment update), ``blocks`` (2000 uneven U(1)
+blocks: grouped vs graph vs plain launches), ``serving`` (a Poisson stream of
+mixed requests: continuous batching vs one request at a time).
 """
 from __future__ import annotations
 
@@ -686,7 +691,7 @@ def main():
     ap.add_argument("--cpu-rows", type=int, default=M)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--profile", action="store_true",
                     help="profiling target: plan, one warm-up execute, --steps executes, exit")
     ap.add_argument("--workload", default="permuted4",
@@ -805,28 +810,59 @@ def main():
     # Dominant kernel's own duration: the plan's GEMM stage, timed alone.
     roof, stages = roofline(plan, stage_ms, nexec)
 
-    # End to end through the public API with host buffers.
+    # End to end through the public API with host buffers: every step copies
+    # its A, B and C from pinned host memory and its C back.  Steps are
+    # pipelined the way a caller streaming contractions would run them: two
+    # device buffer sets (a plan on each), uploads on one stream, executes on
+    # a second, downloads on a third, so step i+1's upload overlaps step i's
+    # execute and download.
     A_p = torch.from_numpy(A_h).pin_memory()
     B_p = torch.from_numpy(B_h).pin_memory()
     C_p = torch.from_numpy(C_h).pin_memory()
-    C_out = torch.empty_like(C_p).pin_memory()
+    outs = [torch.empty_like(C_p).pin_memory() for _ in range(2)]
     h2d = (A_p.numel() + B_p.numel() + C_p.numel()) * 8
-    d2h = C_out.numel() * 8
-    for _ in range(1):
-        Ad.copy_(A_p, non_blocking=True); Bd.copy_(B_p, non_blocking=True); Cd.copy_(C_p, non_blocking=True)
-        qs.execute(plan, ALPHA, BETA)
-        C_out.copy_(Cd, non_blocking=True)
+    d2h = outs[0].numel() * 8
+    A1d, B1d, C1d = torch.empty_like(Ad), torch.empty_like(Bd), torch.empty_like(Cd)
+    plan1 = qs.plan_contract(qs.StridedView(C1d, sc, colmajor_strides(sc), 0), qs.StridedView(A1d, sa, colmajor_strides(sa), 0),
+                             LABELS["indA"], qs.StridedView(B1d, sb, colmajor_strides(sb), 0), LABELS["indB"],
+                             LABELS["indC"], method=args.method, per_product_gemm=args.per_product)
+    bufs = [(Ad, Bd, Cd, plan), (A1d, B1d, C1d, plan1)]
+    s_in, s_run, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_run = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_step(i):
+        a_d, b_d, c_d, p = bufs[i % 2]
+        if i >= 2:
+            s_in.wait_event(ev_out[i % 2])   # buffer set free: step i-2 fully done
+        with torch.cuda.stream(s_in):
+            a_d.copy_(A_p, non_blocking=True)
+            b_d.copy_(B_p, non_blocking=True)
+            c_d.copy_(C_p, non_blocking=True)
+            ev_in[i % 2].record(s_in)
+        s_run.wait_event(ev_in[i % 2])
+        qs.execute(p, ALPHA, BETA, stream=s_run)
+        ev_run[i % 2].record(s_run)
+        s_out.wait_event(ev_run[i % 2])
+        with torch.cuda.stream(s_out):
+            outs[i % 2].copy_(c_d, non_blocking=True)
+            ev_out[i % 2].record(s_out)
+
+    for i in range(2):
+        e2e_step(i)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        Ad.copy_(A_p, non_blocking=True); Bd.copy_(B_p, non_blocking=True); Cd.copy_(C_p, non_blocking=True)
-        qs.execute(plan, ALPHA, BETA)
-        C_out.copy_(Cd, non_blocking=True)
-    e1.record(stream)
+    e0.record(s_in)
+    s_run.wait_event(e0)
+    s_out.wait_event(e0)
+    for i in range(args.e2e_steps):
+        e2e_step(i)
+    e1.record(s_out)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.e2e_steps, world, dev)
     e2e_value = world * FLOPS / (e2e_ms * 1e-3) / 1e12
+    plan1.release()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -854,7 +890,8 @@ def main():
             "roofline": roof, "stages_ms": stages,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": args.e2e_steps,
+                    "pipelined": "uploads, executes and downloads on three streams, two buffer sets"},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }), flush=True)
