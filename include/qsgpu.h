@@ -244,6 +244,18 @@ int qs_group_destroy(qs_group *g);
 int qs_execute_grouped(int32_t n, qs_plan *const *plans, const double *alpha,
                        const double *beta, void *stream);
 
+/* TO.tensoradd! / TO.tensortrace! on the device, which the reference forwards
+ * to StridedNative on the host (src/integrations/tensoroperations.jl:90-107):
+ *   C[indC] = alpha * sum over traced labels of op(A)[indA] + beta * C[indC]
+ * Every label of indC appears exactly once in indA (a permutation: tensoradd!);
+ * every other label of indA appears exactly twice (a traced pair:
+ * tensortrace!).  conjA is XORed with A's op; a conjugated C is rejected.
+ * beta == 0 never reads C, alpha == 0 never reads A; bounds are checked
+ * before any launch.  One kernel on `stream`; allocates nothing. */
+int qs_tensoradd_trace(const qs_view *C, const double *alpha, const qs_view *A,
+                       const int64_t *indA, int32_t conjA, const double *beta,
+                       const int64_t *indC, void *stream);
+
 /* contract! without any device allocation.  No counterpart in the reference:
  * it is for callers that cannot allocate device memory when they contract,
  * e.g. a serving loop where cudaMalloc/cudaFree would synchronize the device

@@ -37,7 +37,7 @@ __all__ = [
     "StridedView", "plan_contract", "execute", "contract", "ContractPlan", "PathModes",
     "QuasiStridedBackend", "tensorcontract", "contraction_labels", "release",
     "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "colmajor",
-    "execute_grouped", "ContractGroup",
+    "execute_grouped", "ContractGroup", "add_trace", "tensoradd", "tensortrace",
 ]
 
 _DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
@@ -486,6 +486,58 @@ class QuasiStridedBackend:
 
     def __repr__(self):
         return f"QuasiStridedBackend(accumulator={self.accumulator})"
+
+
+def add_trace(C: StridedView, alpha, A: StridedView, indA, beta, indC, *, conjA=False, stream=None):
+    """C[indC] = alpha * sum over the traced labels of op(A)[indA] + beta * C
+    on the device (qs_tensoradd_trace): labels of indC appear once in indA,
+    the other labels of indA exactly twice (traced pairs)."""
+    _check_device(False, C, A, A)
+    keep: list = []
+    cC, cA = C._c(keep), A._c(keep)
+    iA = _labels(indA, A.ndim, "indA", keep)
+    iC = _labels(indC, C.ndim, "indC", keep)
+    _abi.check(_abi.lib().qs_tensoradd_trace(ctypes.byref(cC), _scalar(alpha), ctypes.byref(cA), iA,
+                                             int(bool(conjA)), _scalar(beta), iC, _stream_ptr(stream)))
+    return C
+
+
+def _as_view(x):
+    return x if isinstance(x, StridedView) else StridedView(x)
+
+
+def tensoradd(C, A, pA, conjA, alpha, beta, backend: "QuasiStridedBackend" = None, allocator=None):
+    """``TO.tensoradd!(C, A, pA, conjA, α, β, backend)``: C = β C + α
+    permutedims(op(A), linearize(pA)), on the device (the reference forwards
+    this to StridedNative on the host)."""
+    Cv, Av = _as_view(C), _as_view(A)
+    perm = tuple(pA[0]) + tuple(pA[1])
+    if sorted(perm) != list(range(1, Av.ndim + 1)) or len(perm) != Cv.ndim:
+        raise ArgumentError("tensoradd: pA must be a permutation of A's axes with one entry per axis of C")
+    indA = [0] * Av.ndim
+    for i, ax in enumerate(perm):
+        indA[ax - 1] = i + 1
+    add_trace(Cv, alpha, Av, tuple(indA), beta, tuple(range(1, Cv.ndim + 1)), conjA=conjA)
+    return C
+
+
+def tensortrace(C, A, p, q, conjA, alpha, beta, backend: "QuasiStridedBackend" = None, allocator=None):
+    """``TO.tensortrace!(C, A, p, q, conjA, α, β, backend)``: C = β C + α
+    (partial trace of op(A) over the axis pairs (q[1][j], q[2][j]),
+    remaining axes linearize(p) in C's order), on the device."""
+    Cv, Av = _as_view(C), _as_view(A)
+    keep_ax = tuple(p[0]) + tuple(p[1])
+    q1, q2 = tuple(q[0]), tuple(q[1])
+    if len(q1) != len(q2) or len(keep_ax) != Cv.ndim or \
+            sorted(keep_ax + q1 + q2) != list(range(1, Av.ndim + 1)):
+        raise ArgumentError("tensortrace: p and q must partition A's axes (q as pairs), p one per axis of C")
+    indA = [0] * Av.ndim
+    for i, ax in enumerate(keep_ax):
+        indA[ax - 1] = i + 1
+    for j, (x, y) in enumerate(zip(q1, q2)):
+        indA[x - 1] = indA[y - 1] = -(j + 1)
+    add_trace(Cv, alpha, Av, tuple(indA), beta, tuple(range(1, Cv.ndim + 1)), conjA=conjA)
+    return C
 
 
 def tensorcontract(C, A, pA, conjA, B, pB, conjB, pAB, alpha, beta,

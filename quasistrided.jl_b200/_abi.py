@@ -142,6 +142,8 @@ SIGNATURES = {
     "qs_contract_noalloc": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
                                            ctypes.POINTER(qs_view), _I64P, _DP, _I64P,
                                            ctypes.POINTER(qs_plan_options), _P]),
+    "qs_tensoradd_trace": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
+                                          ctypes.c_int32, _DP, _I64P, _P]),
     "qs_version": (ctypes.c_char_p, []),
 }
 

@@ -274,7 +274,7 @@ int check_bounds(const qs_plan *p, bool reads_ab) {
   return QS_OK;
 }
 
-static int validate_view(const qs_view *v, const char *name) {
+int validate_view(const qs_view *v, const char *name) {
   if (!v) return fail(QS_EINVAL, std::string("ArgumentError: ") + name + " is NULL");
   if (v->ndim < 0 || v->ndim > 64)
     return fail(QS_EINVAL, std::string("ArgumentError: ") + name + " has an invalid rank");

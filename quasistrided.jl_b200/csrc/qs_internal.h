@@ -145,6 +145,8 @@ int device_alloc(void **p, size_t bytes);
 void device_free_all(std::vector<void *> &ptrs);
 
 // planner.cpp
+// Shape, eltype and op checks of one view (QS_EINVAL with a message).
+int validate_view(const qs_view *v, const char *name);
 int plan_host(qs_plan *p, const qs_view *C, const qs_view *A,
               const int64_t *indA, const qs_view *B, const int64_t *indB,
               const int64_t *indC, const qs_plan_options *opts);
