@@ -182,4 +182,55 @@ function TO.tensorcontract!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::B
     return C
 end
 
+"""
+    add_trace!(C, alpha, A, indA, beta, indC; conjA = false) -> C
+
+`C[indC] = alpha * (sum over traced labels of op(A)[indA]) + beta * C` on the
+device (qs_tensoradd_trace): labels of indC appear once in indA, the other
+labels of indA exactly twice. Runs on CUDA.jl's current stream.
+"""
+function add_trace!(C::DeviceStridedView, alpha::Number, A::DeviceStridedView, indA, beta::Number, indC;
+        conjA::Bool = false)
+    keep = Any[]
+    cC, cA = cview(C, keep), cview(A, keep)
+    iA, iC = collect(Int64, indA), collect(Int64, indC)
+    GC.@preserve keep iA iC begin
+        check(ccall((:qs_tensoradd_trace, libqsgpu), Cint,
+            (Ref{QSView}, Ptr{Float64}, Ref{QSView}, Ptr{Int64}, Int32, Ptr{Float64}, Ptr{Int64}, Ptr{Cvoid}),
+            cC, Float64[real(alpha), imag(alpha)], cA, iA, Int32(conjA), Float64[real(beta), imag(beta)], iC,
+            reinterpret(Ptr{Cvoid}, CUDA.stream().handle)))
+    end
+    return C
+end
+
+# TO.tensoradd!: C = β C + α permutedims(op(A), linearize(pA)); the reference
+# forwards this to StridedNative on the host (tensoroperations.jl:91-98).
+function TO.tensoradd!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::Bool, α::Number, β::Number,
+        ::QuasiStridedGPUBackend, allocator = TO.DefaultAllocator())
+    perm = (pA[1]..., pA[2]...)
+    indA = zeros(Int64, ndims(A))
+    for (i, ax) in enumerate(perm)
+        indA[ax] = i
+    end
+    add_trace!(DeviceStridedView(C), α, DeviceStridedView(A), indA, β, 1:ndims(C); conjA)
+    CUDA.synchronize()
+    return C
+end
+
+# TO.tensortrace!: C = β C + α (trace of op(A) over the pairs (q[1][j], q[2][j]),
+# the kept axes linearize(p) in C's order) (tensoroperations.jl:100-107).
+function TO.tensortrace!(C::CuArray, A::CuArray, p::TO.Index2Tuple, q::TO.Index2Tuple, conjA::Bool,
+        α::Number, β::Number, ::QuasiStridedGPUBackend, allocator = TO.DefaultAllocator())
+    indA = zeros(Int64, ndims(A))
+    for (i, ax) in enumerate((p[1]..., p[2]...))
+        indA[ax] = i
+    end
+    for (j, (x, y)) in enumerate(zip(q[1], q[2]))
+        indA[x] = indA[y] = -j
+    end
+    add_trace!(DeviceStridedView(C), α, DeviceStridedView(A), indA, β, 1:ndims(C); conjA)
+    CUDA.synchronize()
+    return C
+end
+
 end # module
