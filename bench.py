@@ -589,7 +589,8 @@ def run_matmul(args):
     """The permuted matmul C[a,n,b] = sum_k A[a,k,b] * B[k,n] (a=96, k=128,
     b=32, n=80; alpha = 1, beta = 0; M = (a,b) is not contiguous in C), in
     Float64: microseconds per call for execute on a reused plan, the same
-    replayed as a CUDA graph, and one-shot contract (plan, execute, release).
+    replayed as a CUDA graph, and one-shot contract (plan, execute, release)
+    with the workspace from the library's pool and from a device arena.
     Launch-latency bound (63 MFLOP).  Prints one JSON line."""
     import torch
     qs = load_engine()
@@ -628,6 +629,13 @@ def run_matmul(args):
     res["graph_us"], res["graph_host_us"] = timed(lambda: qs.execute(gplan, 1.0, 0.0), steps)
     res["contract_us"], res["contract_host_us"] = timed(
         lambda: qs.contract(Cv, 1.0, Av, labels[0], Bv, labels[1], 0.0, labels[2]), max(args.steps, 50))
+    # One-shot contract with the workspace from a device arena (no cudaMalloc,
+    # no wait for the stream; checkpoint/reset around each call).
+    arena = qs.DeviceArena(64 << 20)
+    res["contract_arena_us"], res["contract_arena_host_us"] = timed(
+        lambda: qs.contract(Cv, 1.0, Av, labels[0], Bv, labels[1], 0.0, labels[2], allocator=arena),
+        max(args.steps, 50))
+    res["arena_waits"] = arena.info()["waits"]
     qs.execute(plan, 1.0, 0.0)
     torch.cuda.synchronize()
     got = Cd.cpu().numpy()

@@ -115,6 +115,25 @@ typedef struct qs_view {
   int32_t reserved;
 } qs_view;
 
+/* A device allocator for plan workspace: TensorOperations' `allocator`
+ * argument of plan_contract (src/planning/plan.jl:115-133), whose
+ * ContractWorkspace takes its panels with tensoralloc and hands them back with
+ * tensorfree! in reverse order (src/execution/workspace.jl:98-123).
+ *   alloc: at least `bytes` bytes of device memory on the current device,
+ *          aligned to 256 bytes, free for work enqueued after the call on any
+ *          stream; NULL when it has none (the plan then fails with QS_ENOMEM).
+ *   free:  hands a block back; a plan's blocks come back in the reverse order
+ *          of allocation.  `stream` is the stream of the plan's last execute
+ *          (NULL: the legacy default stream); work on it that used the block
+ *          may still be running, so an allocator that reuses the block orders
+ *          the reuse after that work (the built-in qs_arena does).
+ * The plan keeps a copy of this struct; `ctx` must outlive the plan. */
+typedef struct qs_allocator {
+  void *ctx;
+  void *(*alloc)(void *ctx, size_t bytes);
+  void (*free)(void *ctx, void *ptr, size_t bytes, void *stream);
+} qs_allocator;
+
 typedef struct qs_plan_options {
   int32_t conjA;       /* conjugate A's elements (XOR with A's op) */
   int32_t conjB;       /* conjugate B's elements (XOR with B's op) */
@@ -132,6 +151,8 @@ typedef struct qs_plan_options {
   int32_t native_tile;     /* gather-GEMM tile: 0 = by M and N; 1 = 64x64, 2 = 128x32,
                               3 = 256x16, 4 = 32x32 (real compute types; the
                               autotuner's knob) */
+  const qs_allocator *allocator; /* plan workspace from here; NULL = the library's
+                                    stream-ordered pool (DefaultAllocator) */
 } qs_plan_options;
 
 typedef struct qs_plan_info {
@@ -169,7 +190,10 @@ int qs_execute(qs_plan *plan, const double *alpha, const double *beta,
                void *stream);
 
 /* contract! (src/execution/execute.jl:264-275): plan, execute, release in one
- * call.  The plan's workspace is freed stream-ordered after the work. */
+ * call.  The plan's workspace is freed stream-ordered after the work: with
+ * the library's pool the call waits for `stream`; with opts->allocator it
+ * returns once the work is enqueued and hands the workspace back with
+ * `stream` (the allocator orders its reuse, as the qs_arena does). */
 int qs_contract(const qs_view *C, const double *alpha, const qs_view *A,
                 const int64_t *indA, const qs_view *B, const int64_t *indB,
                 const double *beta, const int64_t *indC,
@@ -287,6 +311,38 @@ int qs_plan_stage_times(qs_plan *plan, double *stage_ms, int32_t max_stages,
  * returns QS_ETIMEOUT (and clears the word) if a bounded wait gave up since
  * the last check, else QS_OK. */
 int qs_plan_check_status(qs_plan *plan, void *stream);
+
+/* Device arena: the device counterpart of TensorOperations' BufferAllocator
+ * (the allocators plan_contract accepts; checkpoint/reset bracket every
+ * TO.tensorcontract!, src/integrations/tensoroperations.jl:84-86).  A bump
+ * allocator over one device buffer: O(1) allocation with no cudaMalloc and
+ * no synchronization, blocks handed back LIFO, everything above a checkpoint
+ * reclaimed by a reset.  Memory that a free or a reset hands back is reused
+ * only after the work enqueued before it on the given stream is done (the
+ * allocation that reuses it waits on an event).  Thread-safe.
+ *   create:     base == NULL allocates `bytes` with cudaMalloc on the current
+ *               device (freed by destroy); otherwise the arena serves the
+ *               caller's device memory [base, base+bytes) (a CuArray, a torch
+ *               tensor), which must outlive it.
+ *   allocator:  the qs_allocator to put in qs_plan_options.allocator.
+ *   alloc/free: tensoralloc / tensorfree! of intermediates (256-byte aligned;
+ *               QS_ENOMEM when the arena is full).  free of the top block pops
+ *               it (and any freed blocks under it); of another block marks it;
+ *               of a block a reset already reclaimed does nothing.
+ *   checkpoint: allocator_checkpoint! (the current top, in bytes).
+ *   reset:      allocator_reset!: drops every block above `checkpoint`; `stream`
+ *               is where the work that used them was enqueued. */
+typedef struct qs_arena qs_arena;
+int qs_arena_create(qs_arena **arena, void *base, size_t bytes);
+int qs_arena_destroy(qs_arena *arena);
+const qs_allocator *qs_arena_allocator(qs_arena *arena);
+int qs_arena_alloc(qs_arena *arena, size_t bytes, void **out);
+int qs_arena_free(qs_arena *arena, void *ptr, size_t bytes, void *stream);
+size_t qs_arena_checkpoint(qs_arena *arena);
+int qs_arena_reset(qs_arena *arena, size_t checkpoint, void *stream);
+/* used = current top, peak = highest top since create, capacity = bytes,
+ * waits = allocations that had to wait for reclaimed memory's work. */
+int qs_arena_get_info(qs_arena *arena, size_t *used, size_t *peak, size_t *capacity, int64_t *waits);
 
 /* Number of device kernels this library has launched in this process
  * (instrumentation: benchmarks difference it around a timed region). */

@@ -30,6 +30,8 @@ from typing import Optional, Sequence
 import torch
 
 from . import _abi
+from .allocators import (DeviceArena, TorchAllocator, allocator_checkpoint,  # noqa: F401
+                         allocator_handle, allocator_reset, tensoralloc, tensorfree)
 from ._abi import (ArgumentError, BoundsError, DimensionMismatch, EngineError,  # noqa: F401
                    QS_C32, QS_C64, QS_F32, QS_F64)
 
@@ -38,6 +40,8 @@ __all__ = [
     "QuasiStridedBackend", "tensorcontract", "contraction_labels", "release",
     "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "colmajor",
     "execute_grouped", "ContractGroup", "add_trace", "tensoradd", "tensortrace",
+    "DeviceArena", "TorchAllocator", "tensoralloc", "tensorfree", "allocator_checkpoint",
+    "allocator_reset",
 ]
 
 _DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
@@ -306,9 +310,10 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     device work.  ``kernel`` names a method ("native", "ozaki", "bf16x3");
     ``cuda_graph`` makes ``execute`` replay a captured CUDA graph of the
     plan's launches (re-captured when alpha/beta change);
-    ``allocator`` is accepted for signature parity (the plan allocates its
-    workspace in device memory).  ``host_only`` plans without touching the
-    device (inspection only).
+    ``allocator`` serves the plan's device workspace (None: the library's
+    pool; a ``DeviceArena`` or ``TorchAllocator``), handed back in reverse
+    order by ``release``; it must outlive the plan.  ``host_only`` plans
+    without touching the device (inspection only).
     """
     if kernel is not None:
         method = kernel
@@ -321,11 +326,13 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
                  ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph)
     o.native_tile = int(native_tile)
+    o.allocator = None if host_only else allocator_handle(allocator)
     h = ctypes.c_void_p()
     _abi.check(_abi.lib().qs_plan_contract(ctypes.byref(h), ctypes.byref(cC), ctypes.byref(cA), iA,
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))
     plan = ContractPlan(h, C, A, B, host_only)
     plan.per_product_gemm, plan.cuda_graph = bool(per_product_gemm), bool(cuda_graph)
+    plan.allocator = allocator
     return plan
 
 
@@ -378,8 +385,12 @@ def release(plan: ContractPlan, allocator=None) -> None:
 
 
 def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, beta, indC, *,
-             accumulator=None, conjA=False, conjB=False, method="auto", stream=None) -> StridedView:
-    """``contract!``: plan, execute, release; returns C."""
+             accumulator=None, conjA=False, conjB=False, method="auto", stream=None,
+             allocator=None) -> StridedView:
+    """``contract!``: plan, execute, release; returns C.  With the library's
+    pool this waits for the stream; with an ``allocator`` it returns once the
+    work is enqueued (a ``DeviceArena`` is bracketed by checkpoint/reset, as
+    TO.tensorcontract! brackets its allocator)."""
     _check_device(False, C, A, B)
     keep: list = []
     cC, cA, cB = C._c(keep), A._c(keep), B._c(keep)
@@ -387,9 +398,15 @@ def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, 
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method)
-    _abi.check(_abi.lib().qs_contract(ctypes.byref(cC), _scalar(alpha), ctypes.byref(cA), iA,
-                                      ctypes.byref(cB), iB, _scalar(beta), iC, ctypes.byref(o),
-                                      _stream_ptr(stream)))
+    o.allocator = allocator_handle(allocator)
+    cp = allocator_checkpoint(allocator)
+    try:
+        _abi.check(_abi.lib().qs_contract(ctypes.byref(cC), _scalar(alpha), ctypes.byref(cA), iA,
+                                          ctypes.byref(cB), iB, _scalar(beta), iC, ctypes.byref(o),
+                                          _stream_ptr(stream)))
+    finally:
+        if cp is not None:
+            allocator_reset(allocator, cp, stream)
     return C
 
 
@@ -552,5 +569,5 @@ def tensorcontract(C, A, pA, conjA, B, pB, conjB, pAB, alpha, beta,
     indA, indB, indC = contraction_labels(pA, pB, pAB)
     # dimcheck_tensorcontract: matching extents are checked by the planner.
     contract(Cv, alpha, Av, indA, Bv, indB, beta, indC, accumulator=backend.accumulator,
-             conjA=conjA, conjB=conjB)
+             conjA=conjA, conjB=conjB, allocator=allocator)
     return C

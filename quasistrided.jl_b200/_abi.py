@@ -67,6 +67,19 @@ class qs_plan_options(ctypes.Structure):
         ("complex_mode", ctypes.c_int32),
         ("flags", ctypes.c_int32),
         ("native_tile", ctypes.c_int32),
+        ("allocator", ctypes.c_void_p),
+    ]
+
+
+ALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+FREE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+
+
+class qs_allocator(ctypes.Structure):
+    _fields_ = [
+        ("ctx", ctypes.c_void_p),
+        ("alloc", ALLOC_FN),
+        ("free", FREE_FN),
     ]
 
 
@@ -145,6 +158,15 @@ SIGNATURES = {
     "qs_tensoradd_trace": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
                                           ctypes.c_int32, _DP, _I64P, _P]),
     "qs_version": (ctypes.c_char_p, []),
+    "qs_arena_create": (ctypes.c_int, [ctypes.POINTER(_P), _P, ctypes.c_size_t]),
+    "qs_arena_destroy": (ctypes.c_int, [_P]),
+    "qs_arena_allocator": (_P, [_P]),
+    "qs_arena_alloc": (ctypes.c_int, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "qs_arena_free": (ctypes.c_int, [_P, _P, ctypes.c_size_t, _P]),
+    "qs_arena_checkpoint": (ctypes.c_size_t, [_P]),
+    "qs_arena_reset": (ctypes.c_int, [_P, ctypes.c_size_t, _P]),
+    "qs_arena_get_info": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                         ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int64)]),
 }
 
 _lib = None

@@ -40,6 +40,26 @@ static cudaStream_t setup_stream(cudaError_t *err) {
   return s;
 }
 
+void *plan_setup_stream() {
+  cudaError_t e = cudaSuccess;
+  return (void *)setup_stream(&e);
+}
+
+int setup_upload(void *dst, const void *src, size_t bytes) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  if (e != cudaSuccess) return (int)e;
+  // From pageable memory the call returns once `src` is staged: no wait.
+  return (int)cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+}
+
+int setup_zero_async(void *dst, size_t bytes) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  if (e != cudaSuccess) return (int)e;
+  return (int)cudaMemsetAsync(dst, 0, bytes, s);
+}
+
 int setup_copy(void *dst, const void *src, size_t bytes, int to_device) {
   cudaError_t e = cudaSuccess;
   cudaStream_t s = setup_stream(&e);
@@ -65,9 +85,8 @@ int device_alloc(void **p, size_t bytes) {
     }
     pool_dev = cur;
   }
-  e = cudaMallocAsync(p, bytes, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  return (int)e;
+  // Stream-ordered: the plan's ready event orders every later use.
+  return (int)cudaMallocAsync(p, bytes, s);
 }
 
 void device_free_all(std::vector<void *> &ptrs) {
@@ -78,6 +97,81 @@ void device_free_all(std::vector<void *> &ptrs) {
   for (void *q : ptrs) cudaFreeAsync(q, s);
   cudaStreamSynchronize(s);
   ptrs.clear();
+}
+
+int plan_alloc(qs_plan *p, void **out, size_t bytes) {
+  *out = nullptr;
+  if (p->has_alloc) {
+    if (is_arena_allocator(&p->alloc)) {
+      // Reuse of reclaimed arena memory waits on the setup stream, not the host.
+      int rc = arena_alloc_ordered(p->alloc.ctx, bytes, out, plan_setup_stream());
+      if (rc) {
+        *out = nullptr;
+        return rc;
+      }
+    } else {
+      *out = p->alloc.alloc(p->alloc.ctx, bytes);
+    }
+    if (!*out) {
+      std::ostringstream s;
+      s << "the plan's allocator has no " << bytes << " bytes of device memory";
+      return fail(QS_ENOMEM, s.str());
+    }
+  } else {
+    cudaError_t e = (cudaError_t)device_alloc(out, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *out = nullptr;
+      std::ostringstream s;
+      s << "device allocation of " << bytes << " bytes failed: " << cudaGetErrorString(e);
+      return fail(QS_ENOMEM, s.str());
+    }
+  }
+  p->ws.owned.push_back(*out);
+  p->ws.owned_bytes.push_back(bytes);
+  p->ws.bytes += bytes;
+  return QS_OK;
+}
+
+void plan_mark_ready(qs_plan *p) {
+  cudaError_t e = cudaSuccess;
+  cudaStream_t s = setup_stream(&e);
+  cudaEvent_t ev = nullptr;
+  if (e == cudaSuccess && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess &&
+      cudaEventRecord(ev, s) == cudaSuccess) {
+    p->ready = (void *)ev;
+    return;
+  }
+  cudaGetLastError();
+  if (ev) cudaEventDestroy(ev);
+  cudaStreamSynchronize(s);  // no event: finish the setup now
+}
+
+void plan_sync_ready(qs_plan *p) {
+  if (!p->ready) return;
+  cudaEventSynchronize((cudaEvent_t)p->ready);
+  cudaEventDestroy((cudaEvent_t)p->ready);
+  p->ready = nullptr;
+}
+
+void plan_wait_ready(qs_plan *p, void *stream) {
+  if (!p->ready) return;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t ev = (cudaEvent_t)p->ready;
+  if (cudaEventQuery(ev) == cudaSuccess) {
+    cudaEventDestroy(ev);
+    p->ready = nullptr;
+    return;
+  }
+  cudaGetLastError();  // cudaErrorNotReady is not a failure
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    // A capture cannot wait on an event recorded outside it: finish now.
+    cudaGetLastError();
+    plan_sync_ready(p);
+    return;
+  }
+  cudaStreamWaitEvent(st, ev, 0);
 }
 
 int setup_zero(void *dst, size_t bytes) {
@@ -138,40 +232,62 @@ int cuda_fail(cudaError_t e, const char *what) {
 }
 
 void free_workspace(qs_plan *p) {
-  device_free_all(p->ws.owned);
+  if (p->has_alloc) {
+    // Back to the caller's allocator in reverse order (release!,
+    // src/execution/workspace.jl:118-123).  A grouped plan's last work may
+    // be on a group's side streams, which the allocator cannot see: wait.
+    if (p->grouped) {
+      cudaDeviceSynchronize();
+    } else if (!p->executed) {
+      cudaError_t e = cudaSuccess;
+      cudaStreamSynchronize(setup_stream(&e));  // plan-time uploads may be in flight
+    }
+    for (size_t i = p->ws.owned.size(); i-- > 0;)
+      p->alloc.free(p->alloc.ctx, p->ws.owned[i], p->ws.owned_bytes[i], p->grouped ? nullptr : p->last_stream);
+    p->ws.owned.clear();
+  } else {
+    device_free_all(p->ws.owned);
+  }
   p->ws = Workspace{};
 }
 
 int ws_alloc(qs_plan *p, void **out, size_t bytes) {
   *out = nullptr;
   if (bytes == 0) return QS_OK;
-  cudaError_t e = (cudaError_t)device_alloc(out, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    std::ostringstream s;
-    s << "device allocation of " << bytes << " bytes failed: " << cudaGetErrorString(e);
-    return fail(QS_ENOMEM, s.str());
-  }
-  p->ws.owned.push_back(*out);
-  p->ws.bytes += bytes;
-  return QS_OK;
+  return plan_alloc(p, out, bytes);
 }
 
-int upload_offsets(qs_plan *p, const Group &g, int64_t **dst) {
-  int64_t Q = g.length();
-  size_t n = (size_t)(Q > 0 ? Q : 1);
-  std::vector<int64_t> h(2 * n, 0);
-  if (Q > 0) {
-    g.fill_offsets(0, 0, Q, h.data());
-    g.fill_offsets(1, 0, Q, h.data() + n);
+// The M, N and K offset tables (two maps each) in one block and one copy.
+int upload_offsets(qs_plan *p) {
+  const Group *gs[3] = {&p->mg, &p->ng, &p->kg};
+  int64_t **dst[3] = {p->ws.offM, p->ws.offN, p->ws.offK};
+  size_t n[3], total = 0;
+  for (int i = 0; i < 3; ++i) {
+    const int64_t Q = gs[i]->length();
+    n[i] = (size_t)(Q > 0 ? Q : 1);
+    total += 2 * n[i];
+  }
+  std::vector<int64_t> h(total, 0);
+  size_t at = 0;
+  for (int i = 0; i < 3; ++i) {
+    const int64_t Q = gs[i]->length();
+    if (Q > 0) {
+      gs[i]->fill_offsets(0, 0, Q, h.data() + at);
+      gs[i]->fill_offsets(1, 0, Q, h.data() + at + n[i]);
+    }
+    at += 2 * n[i];
   }
   void *d;
-  int rc = ws_alloc(p, &d, 2 * n * sizeof(int64_t));
+  int rc = ws_alloc(p, &d, total * sizeof(int64_t));
   if (rc) return rc;
-  cudaError_t e = (cudaError_t)setup_copy(d, h.data(), 2 * n * sizeof(int64_t), 1);
+  cudaError_t e = (cudaError_t)setup_upload(d, h.data(), total * sizeof(int64_t));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (offset tables)");
-  dst[0] = (int64_t *)d;
-  dst[1] = (int64_t *)d + n;
+  at = 0;
+  for (int i = 0; i < 3; ++i) {
+    dst[i][0] = (int64_t *)d + at;
+    dst[i][1] = (int64_t *)d + at + n[i];
+    at += 2 * n[i];
+  }
   return QS_OK;
 }
 
@@ -280,6 +396,16 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
     delete p;
     return rc;
   }
+  if (p->opts.allocator) {
+    const qs_allocator *al = p->opts.allocator;
+    if (!al->alloc || !al->free) {
+      delete p;
+      return fail(QS_EINVAL, "ArgumentError: a qs_allocator needs both alloc and free");
+    }
+    p->alloc = *al;
+    p->has_alloc = 1;
+    p->opts.allocator = nullptr;  // the copy above is what the plan keeps
+  }
   if (p->path == QS_PATH_NEST) {
     rc = choose_method(p);
     if (rc) {
@@ -302,8 +428,7 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
       return cuda_fail(e, "cudaGetDevice");
     }
     if (p->path != QS_PATH_EMPTY) {
-      if ((rc = upload_offsets(p, p->mg, p->ws.offM)) || (rc = upload_offsets(p, p->ng, p->ws.offN)) ||
-          (rc = upload_offsets(p, p->kg, p->ws.offK))) {
+      if ((rc = upload_offsets(p))) {
         free_workspace(p);
         delete p;
         return rc;
@@ -317,6 +442,9 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
         return rc;
       }
     }
+    // The uploads and clears above are still in flight on the setup stream;
+    // every execute waits for this event (qs_execute, groups, graphs).
+    if (!p->ws.owned.empty()) plan_mark_ready(p);
   } else if (p->path == QS_PATH_NEST && p->method != QS_METHOD_NATIVE) {
     tc_geometry(p);
   }
@@ -336,6 +464,11 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
     // NaN alpha is a legal value: it propagates like the reference.
   }
   cudaStream_t st = (cudaStream_t)stream;
+  if (!p->capturing) {
+    plan_wait_ready(p, stream);
+    p->last_stream = stream;
+    p->executed = 1;
+  }
   if ((p->opts.flags & QS_PLAN_CUDA_GRAPH) && !p->capturing) return execute_graph(p, alpha, beta, st);
   int acase = scalar_case(p->T, alpha);
   int bcase = scalar_case(p->T, beta);
@@ -451,6 +584,7 @@ int qs_plan_destroy(qs_plan *p) {
     if (p->cap_stream) cudaStreamDestroy((cudaStream_t)p->cap_stream);
     p->cap_stream = nullptr;
     free_workspace(p);
+    plan_sync_ready(p);
     cudaSetDevice(dev);
   }
   delete p;
@@ -467,8 +601,11 @@ int qs_contract(const qs_view *C, const double *alpha, const qs_view *A, const i
   int rc = qs_plan_contract(&p, C, A, indA, B, indB, indC, &o);
   if (rc) return rc;
   rc = qs_execute(p, alpha, beta, stream);
-  // The workspace is released once the enqueued work is done.
-  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  // The workspace is released once the enqueued work is done: by waiting
+  // here, or, with a caller's allocator, by the allocator ordering its reuse
+  // after `stream`.
+  p->last_stream = stream;
+  cudaError_t e = p->has_alloc ? cudaGetLastError() : cudaStreamSynchronize((cudaStream_t)stream);
   qs_plan_destroy(p);
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");

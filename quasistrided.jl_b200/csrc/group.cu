@@ -283,6 +283,10 @@ int qs_group_create(int32_t n, qs_plan *const *plans, int32_t mode, qs_group **o
   if (!g) return fail(QS_ENOMEM, "host allocation failed");
   g->mode = mode;
   g->plans.assign(plans, plans + n);
+  for (int i = 0; i < n; ++i) {
+    plans[i]->grouped = 1;      // frees of its workspace wait for the device
+    plan_sync_ready(plans[i]);  // group launches and captures need its setup done
+  }
   *out = g;
   return QS_OK;
 }

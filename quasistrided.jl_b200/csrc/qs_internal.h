@@ -73,7 +73,8 @@ struct Workspace {
   int32_t *status = nullptr;  // device status word (bounded waits)
   void *rowmax = nullptr;     // Ozaki: per-row max |x| bit patterns
   size_t bytes = 0;
-  std::vector<void *> owned;  // every cudaMalloc'd pointer, for freeing
+  std::vector<void *> owned;         // every allocated block, for freeing
+  std::vector<size_t> owned_bytes;   // and its size (for a qs_allocator)
 };
 
 struct TensorCoreGeom {
@@ -111,6 +112,18 @@ struct qs_plan {
   int host_only = 0;
   int device = 0;
   qs_plan_options opts{};
+  // Workspace allocator (qs_plan_options.allocator), copied; has_alloc == 0
+  // means the library's stream-ordered pool.  last_stream is the stream of
+  // the last qs_execute (a freed block's work may still run there); grouped
+  // plans may also have run on a group's side streams.
+  qs_allocator alloc{};
+  int has_alloc = 0;
+  void *last_stream = nullptr;
+  int grouped = 0;
+  int executed = 0;
+  // cudaEvent_t recorded on the setup stream after the plan's uploads and
+  // clears; executes wait for it until it has completed (then it is freed).
+  void *ready = nullptr;
   // Per-path launch flags chosen at plan time.
   int a_mfast = 0;  // A's M map is unit-stride (gather along M)
   int b_nfast = 0;  // B's N map is unit-stride (gather along N)
@@ -142,6 +155,21 @@ int setup_zero(void *dst, size_t bytes);
 // never waits for kernels in flight.  Freeing synchronizes the device first:
 // the plan's last executes may still be running on any stream.
 int device_alloc(void **p, size_t bytes);
+// Plan-time device work without host waits: pageable uploads, clears, and
+// the ready event that orders a plan's executes after them.
+void *plan_setup_stream();
+int setup_upload(void *dst, const void *src, size_t bytes);
+int setup_zero_async(void *dst, size_t bytes);
+void plan_mark_ready(qs_plan *p);
+void plan_wait_ready(qs_plan *p, void *stream);  // stream wait (host wait under capture)
+void plan_sync_ready(qs_plan *p);                    // host wait
+// The built-in device arena (arena.cu): recognized so that plan workspace
+// reusing reclaimed memory waits on `stream` instead of the host.
+bool is_arena_allocator(const qs_allocator *a);
+int arena_alloc_ordered(void *ctx, size_t bytes, void **out, void *stream);
+// A block of plan workspace from the plan's allocator (or the pool), recorded
+// in p->ws for freeing; QS_ENOMEM (with the message set) on failure.
+int plan_alloc(qs_plan *p, void **out, size_t bytes);
 void device_free_all(std::vector<void *> &ptrs);
 
 // planner.cpp

@@ -1282,19 +1282,7 @@ void tc_geometry(qs_plan *p) {
   }
 }
 
-static int tc_alloc(qs_plan *p, void **out, size_t bytes) {
-  *out = nullptr;
-  cudaError_t e = (cudaError_t)device_alloc(out, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    std::ostringstream s;
-    s << "device allocation of " << bytes << " bytes failed: " << cudaGetErrorString(e);
-    return fail(QS_ENOMEM, s.str());
-  }
-  p->ws.owned.push_back(*out);
-  p->ws.bytes += bytes;
-  return QS_OK;
-}
+static int tc_alloc(qs_plan *p, void **out, size_t bytes) { return plan_alloc(p, out, bytes); }
 
 int tc_prepare(qs_plan *p) {
   tc_geometry(p);
@@ -1312,14 +1300,14 @@ int tc_prepare(qs_plan *p) {
     int32_t *b = (int32_t *)q;
     p->ws.expA = b;
     p->ws.expB = b + g.Mp;
-    if (setup_zero(q, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
+    if (setup_zero_async(q, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
     p->ws.status = b + n - 1;
     // row/column max bit patterns, cleared per execute
     if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
     p->ws.rowmax = q;
   } else {
     if ((rc = tc_alloc(p, &q, 4 * sizeof(int32_t)))) return rc;
-    if (setup_zero(q, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
+    if (setup_zero_async(q, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
     p->ws.status = (int32_t *)q;
   }
   static bool attr_set[2] = {false, false};
