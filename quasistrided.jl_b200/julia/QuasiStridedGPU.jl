@@ -40,6 +40,7 @@ Base.@kwdef struct QSPlanOptions
     complex_mode::Int32 = 0
     flags::Int32 = 0
     native_tile::Int32 = 0
+    allocator::Ptr{Cvoid} = C_NULL   # const qs_allocator*; C_NULL = the library's pool
 end
 
 const ELTYPE = Dict(Float32 => Int32(0), Float64 => Int32(1), ComplexF32 => Int32(2), ComplexF64 => Int32(3))
@@ -95,7 +96,58 @@ mutable struct ContractPlan
     C::DeviceStridedView
     A::DeviceStridedView
     B::DeviceStridedView
+    allocator::Any   # kept alive while the plan holds its workspace
 end
+
+# --- allocators ---------------------------------------------------------------
+
+"""
+    DeviceArenaAllocator(nbytes)
+
+TensorOperations' BufferAllocator on the device (qs_arena_*): plan workspace
+and `tensoralloc`'d intermediates from one device buffer; `tensorfree!` of the
+last block pops it, `allocator_reset!` reclaims everything after a checkpoint.
+Reclaimed memory is reused only after the work enqueued before the reclaim on
+CUDA.jl's current stream.
+"""
+mutable struct DeviceArenaAllocator
+    handle::Ptr{Cvoid}
+    function DeviceArenaAllocator(nbytes::Integer)
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:qs_arena_create, libqsgpu), Cint, (Ref{Ptr{Cvoid}}, Ptr{Cvoid}, Csize_t),
+            h, C_NULL, nbytes))
+        a = new(h[])
+        finalizer(a) do a
+            a.handle != C_NULL && ccall((:qs_arena_destroy, libqsgpu), Cint, (Ptr{Cvoid},), a.handle)
+            a.handle = C_NULL
+        end
+        return a
+    end
+end
+
+allocator_ptr(::TO.DefaultAllocator) = C_NULL
+allocator_ptr(a::DeviceArenaAllocator) = ccall((:qs_arena_allocator, libqsgpu), Ptr{Cvoid}, (Ptr{Cvoid},), a.handle)
+allocator_ptr(a) = throw(ArgumentError("unsupported allocator $(typeof(a)): use DefaultAllocator or DeviceArenaAllocator"))
+
+curstream() = reinterpret(Ptr{Cvoid}, CUDA.stream().handle)
+
+function TO.tensoralloc(::Type{A}, structure, istemp, a::DeviceArenaAllocator) where {T, N, A <: CuArray{T, N}}
+    p = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:qs_arena_alloc, libqsgpu), Cint, (Ptr{Cvoid}, Csize_t, Ref{Ptr{Cvoid}}),
+        a.handle, prod(structure; init = 1) * sizeof(T), p))
+    return unsafe_wrap(CuArray, CuPtr{T}(UInt(p[])), structure; own = false)
+end
+
+TO.tensorfree!(t::CuArray, a::DeviceArenaAllocator) =
+    (check(ccall((:qs_arena_free, libqsgpu), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Csize_t, Ptr{Cvoid}),
+        a.handle, reinterpret(Ptr{Cvoid}, UInt(pointer(t))), sizeof(t), curstream())); nothing)
+
+TO.allocator_checkpoint!(a::DeviceArenaAllocator) =
+    ccall((:qs_arena_checkpoint, libqsgpu), Csize_t, (Ptr{Cvoid},), a.handle)
+
+TO.allocator_reset!(a::DeviceArenaAllocator, checkpoint) =
+    (check(ccall((:qs_arena_reset, libqsgpu), Cint, (Ptr{Cvoid}, Csize_t, Ptr{Cvoid}),
+        a.handle, checkpoint, curstream())); nothing)
 
 release!(p::ContractPlan) = (p.handle != C_NULL && ccall((:qs_plan_destroy, libqsgpu), Cint, (Ptr{Cvoid},), p.handle); p.handle = C_NULL; nothing)
 
@@ -106,17 +158,19 @@ QuasiStrided.plan_contract for device views (src/planning/plan.jl:115-133).
 """
 function plan_contract(C::DeviceStridedView, A::DeviceStridedView, indA::NTuple{NA, Int},
         B::DeviceStridedView, indB::NTuple{NB, Int}, indC::NTuple{NC, Int};
-        conjA::Bool = false, conjB::Bool = false, accumulator = nothing) where {NA, NB, NC}
+        conjA::Bool = false, conjB::Bool = false, accumulator = nothing,
+        allocator = TO.DefaultAllocator()) where {NA, NB, NC}
     keep = Any[]
     cC, cA, cB = cview(C, keep), cview(A, keep), cview(B, keep)
-    opts = QSPlanOptions(; conjA = Int32(conjA), conjB = Int32(conjB), accumulator = accode(accumulator))
+    opts = QSPlanOptions(; conjA = Int32(conjA), conjB = Int32(conjB), accumulator = accode(accumulator),
+        allocator = allocator_ptr(allocator))
     h = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve keep begin
         check(ccall((:qs_plan_contract, libqsgpu), Cint,
             (Ref{Ptr{Cvoid}}, Ref{QSView}, Ref{QSView}, Ptr{Int64}, Ref{QSView}, Ptr{Int64}, Ptr{Int64}, Ref{QSPlanOptions}),
             h, cC, cA, collect(Int64, indA), cB, collect(Int64, indB), collect(Int64, indC), opts))
     end
-    p = ContractPlan(h[], C, A, B)
+    p = ContractPlan(h[], C, A, B, allocator)
     finalizer(release!, p)
     return p
 end
@@ -174,11 +228,14 @@ function TO.tensorcontract!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::B
     check(ccall((:qs_contraction_labels, libqsgpu), Cint,
         (Int32, Int32, Int32, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}),
         NoA, Nk, NoB, lin(pA), lin(pB), lin(pAB), indA, indB, indC))
+    # Bracketed with checkpoint/reset like the reference (tensoroperations.jl:84-86).
+    checkpoint = TO.allocator_checkpoint!(allocator)
     p = plan_contract(DeviceStridedView(C), DeviceStridedView(A), Tuple(indA), DeviceStridedView(B),
-        Tuple(indB), Tuple(indC); conjA, conjB, accumulator = AC)
+        Tuple(indB), Tuple(indC); conjA, conjB, accumulator = AC, allocator)
     execute!(p, α, β)
-    CUDA.synchronize()
+    allocator isa DeviceArenaAllocator || CUDA.synchronize()
     release!(p)
+    TO.allocator_reset!(allocator, checkpoint)
     return C
 end
 
