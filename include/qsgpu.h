@@ -98,9 +98,13 @@ enum {
   QS_PLAN_PER_PRODUCT_GEMM = 2, /* Ozaki: one slice product per pipeline stage
                                    (the simpler kernel) instead of grouped
                                    diagonals with resident slice tiles */
-  QS_PLAN_CUDA_GRAPH = 4 /* qs_execute captures the plan's launches into a
-                            CUDA graph once (again when alpha/beta change)
-                            and replays it on later calls */
+  QS_PLAN_CUDA_GRAPH = 4, /* qs_execute captures the plan's launches into a
+                             CUDA graph once (again when alpha/beta change)
+                             and replays it on later calls */
+  QS_PLAN_BATCH_LABELS = 8 /* accept labels present in A, B and C (which the
+                              reference rejects, src/planning/labels.jl:48-54)
+                              as batch labels: C[b,...] = alpha * sum_K
+                              A[b,...] B[b,...] + beta * C[b,...] for every b */
 };
 
 typedef struct qs_view {
@@ -172,6 +176,9 @@ typedef struct qs_plan_info {
   int32_t stride_class;  /* bit 0: A's M map unit-stride, bit 1: B's N map,
                             bit 2: C's M map (the autotuner's stride class) */
   int32_t native_tile;   /* gather-GEMM tile in use (1..4 as in the options) */
+  int32_t batch_rank;    /* batch labels (QS_PLAN_BATCH_LABELS), 0 without */
+  int64_t batch_length;  /* product of their extents (1 without) */
+  int64_t batch_labels[16];
 } qs_plan_info;
 
 typedef struct qs_plan qs_plan;

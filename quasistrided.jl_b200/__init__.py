@@ -212,6 +212,8 @@ class ContractPlan:
         self.workspace_bytes = info.workspace_bytes
         self.stride_class = info.stride_class
         self.native_tile = info.native_tile
+        self.batch_labels = tuple(info.batch_labels[:info.batch_rank])
+        self.batch_length = info.batch_length
 
     @property
     def Cstorage(self) -> torch.Tensor:
@@ -259,7 +261,7 @@ class ContractPlan:
 def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=None,
              k_block=None, n_block=None, path_modes: Optional[PathModes] = None,
              ozaki_slices=0, complex_mode=None, host_only=False,
-             per_product_gemm=False, cuda_graph=False) -> _abi.qs_plan_options:
+             per_product_gemm=False, cuda_graph=False, batch_labels=False) -> _abi.qs_plan_options:
     o = _abi.qs_plan_options()
     o.conjA, o.conjB = int(bool(conjA)), int(bool(conjB))
     o.accumulator = _acc_code(accumulator)
@@ -277,7 +279,7 @@ def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=
     o.ozaki_slices = int(ozaki_slices)
     o.complex_mode = _abi.QS_CPLX[complex_mode]
     o.flags = ((_abi.QS_PLAN_HOST_ONLY if host_only else 0) | (2 if per_product_gemm else 0) |
-               (4 if cuda_graph else 0))
+               (4 if cuda_graph else 0) | (_abi.QS_PLAN_BATCH_LABELS if batch_labels else 0))
     return o
 
 
@@ -303,13 +305,15 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                   n_block=None, allocator=None, accumulator=None,
                   path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
                   complex_mode=None, host_only=False, per_product_gemm=False,
-                  cuda_graph=False, native_tile=0) -> ContractPlan:
+                  cuda_graph=False, native_tile=0, batch_labels=False) -> ContractPlan:
     """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
 
     Throws ArgumentError / DimensionMismatch on invalid input, before any
     device work.  ``kernel`` names a method ("native", "ozaki", "bf16x3");
     ``cuda_graph`` makes ``execute`` replay a captured CUDA graph of the
     plan's launches (re-captured when alpha/beta change);
+    ``batch_labels=True`` accepts labels present in A, B and C (the
+    reference rejects them) as batch labels: one contraction per batch entry.
     ``allocator`` serves the plan's device workspace (None: the library's
     pool; a ``DeviceArena`` or ``TorchAllocator``), handed back in reverse
     order by ``release``; it must outlive the plan.  ``host_only`` plans
@@ -324,7 +328,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
-                 ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph)
+                 ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph, batch_labels)
     o.native_tile = int(native_tile)
     o.allocator = None if host_only else allocator_handle(allocator)
     h = ctypes.c_void_p()
@@ -386,7 +390,7 @@ def release(plan: ContractPlan, allocator=None) -> None:
 
 def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, beta, indC, *,
              accumulator=None, conjA=False, conjB=False, method="auto", stream=None,
-             allocator=None) -> StridedView:
+             allocator=None, batch_labels=False) -> StridedView:
     """``contract!``: plan, execute, release; returns C.  With the library's
     pool this waits for the stream; with an ``allocator`` it returns once the
     work is enqueued (a ``DeviceArena`` is bracketed by checkpoint/reset, as
@@ -397,7 +401,7 @@ def contract(C: StridedView, alpha, A: StridedView, indA, B: StridedView, indB, 
     iA = _labels(indA, A.ndim, "indA", keep)
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
-    o = _options(conjA, conjB, accumulator, method)
+    o = _options(conjA, conjB, accumulator, method, batch_labels=batch_labels)
     o.allocator = allocator_handle(allocator)
     cp = allocator_checkpoint(allocator)
     try:

@@ -17,6 +17,7 @@ QS_MODE = {"auto": 0, "never": 1, "always": 2}
 QS_PATH_NAME = {0: "EmptyPath", 1: "ScalePath", 2: "DotPath", 3: "OuterPath", 4: "NestPath"}
 QS_CPLX = {None: 0, "planar": 1, "1m": 2}
 QS_PLAN_HOST_ONLY = 1
+QS_PLAN_BATCH_LABELS = 8
 
 ELTYPE_NAME = {QS_F32: "Float32", QS_F64: "Float64", QS_C32: "ComplexF32", QS_C64: "ComplexF64"}
 
@@ -106,6 +107,9 @@ class qs_plan_info(ctypes.Structure):
         ("workspace_bytes", ctypes.c_int64),
         ("stride_class", ctypes.c_int32),
         ("native_tile", ctypes.c_int32),
+        ("batch_rank", ctypes.c_int32),
+        ("batch_length", ctypes.c_int64),
+        ("batch_labels", ctypes.c_int64 * 16),
     ]
 
 

@@ -207,6 +207,8 @@ Operands make_operands(const qs_plan *p) {
   op.M = p->M;
   op.N = p->N;
   op.K = p->K;
+  op.offBatch = p->ws.offBatch;
+  op.P = p->batched ? p->P : 1;
   return op;
 }
 
@@ -267,6 +269,8 @@ int upload_offsets(qs_plan *p) {
     n[i] = (size_t)(Q > 0 ? Q : 1);
     total += 2 * n[i];
   }
+  const size_t nb = p->batched ? (size_t)p->P : 0;
+  total += 3 * nb;
   std::vector<int64_t> h(total, 0);
   size_t at = 0;
   for (int i = 0; i < 3; ++i) {
@@ -276,6 +280,13 @@ int upload_offsets(qs_plan *p) {
       gs[i]->fill_offsets(1, 0, Q, h.data() + at + n[i]);
     }
     at += 2 * n[i];
+  }
+  if (nb) {
+    // [A | B | C] offsets of every batch entry, first batch label fastest.
+    p->bg.fill_offsets(0, 0, (int64_t)nb, h.data() + at);
+    p->bg.fill_offsets(1, 0, (int64_t)nb, h.data() + at + nb);
+    p->bgc.fill_offsets(0, 0, (int64_t)nb, h.data() + at + 2 * nb);
+    p->batch_host.assign(h.begin() + at, h.begin() + at + 3 * nb);
   }
   void *d;
   int rc = ws_alloc(p, &d, total * sizeof(int64_t));
@@ -288,6 +299,7 @@ int upload_offsets(qs_plan *p) {
     dst[i][1] = (int64_t *)d + at + n[i];
     at += 2 * n[i];
   }
+  p->ws.offBatch = nb ? (int64_t *)d + at : nullptr;
   return QS_OK;
 }
 
@@ -501,7 +513,23 @@ int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream
       if (p->method == QS_METHOD_NATIVE) {
         e = launch_direct(p->T, op, alpha, beta, bcase, p->a_mfast, p->b_nfast, p->native_shape, st);
       } else {
-        int rc2 = tc_execute(p, alpha, beta, bcase, st, ev);
+        int rc2 = QS_OK;
+        if (!p->batched) {
+          rc2 = tc_execute(p, alpha, beta, bcase, st, ev);
+        } else {
+          // One tensor-core pass per batch entry, the operands rebased on
+          // the host; the plan's panels are reused in stream order.
+          const int64_t a0 = p->Abase, b0 = p->Bbase, c0 = p->Cbase, P = p->P;
+          for (int64_t b = 0; b < P && rc2 == QS_OK; ++b) {
+            p->Abase = a0 + p->batch_host[b];
+            p->Bbase = b0 + p->batch_host[P + b];
+            p->Cbase = c0 + p->batch_host[2 * P + b];
+            rc2 = tc_execute(p, alpha, beta, bcase, st, b == 0 ? ev : nullptr);
+          }
+          p->Abase = a0;
+          p->Bbase = b0;
+          p->Cbase = c0;
+        }
         if (rc2 == QS_OK && ev) ++p->prof_nexec;
         return rc2;
       }
@@ -636,6 +664,9 @@ int qs_plan_get_info(const qs_plan *p, qs_plan_info *info) {
   info->workspace_bytes = (int64_t)p->ws.bytes;
   info->stride_class = (p->a_mfast ? 1 : 0) | (p->b_nfast ? 2 : 0) | (p->c_mfast ? 4 : 0);
   info->native_tile = p->native_shape + 1;
+  info->batch_rank = p->batched ? p->bg.D : 0;
+  info->batch_length = p->batched ? p->P : 1;
+  for (int d = 0; d < p->bg.D && d < 16; ++d) info->batch_labels[d] = p->bg.label[d];
   return QS_OK;
 }
 

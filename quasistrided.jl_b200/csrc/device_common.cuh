@@ -33,7 +33,22 @@ struct Operands {
   int conjA, conjB;
   const int64_t *offMA, *offMC, *offNB, *offNC, *offKA, *offKB;
   int64_t M, N, K;
+  // Batch labels: entry b adds offBatch[b], [P + b], [2P + b] to the A, B and
+  // C bases (nullptr and P = 1 without batch labels).
+  const int64_t *offBatch = nullptr;
+  int64_t P = 1;
 };
+
+// The operands of batch entry b.
+__device__ __forceinline__ Operands batch_entry(const Operands &op, int64_t b) {
+  Operands o = op;
+  if (op.offBatch) {
+    o.Abase += op.offBatch[b];
+    o.Bbase += op.offBatch[op.P + b];
+    o.Cbase += op.offBatch[2 * op.P + b];
+  }
+  return o;
+}
 
 // Stored element (any supported eltype) -> real compute type.
 template <class R>

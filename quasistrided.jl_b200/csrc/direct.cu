@@ -24,9 +24,10 @@ namespace qs {
 
 template <class T>
 __global__ void scale_kernel(Operands op, Scalars<T> s, int mfast) {
-  int64_t total = op.M * op.N;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t mn = op.M * op.N, total = mn * op.P;
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < total;
+       f += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = f / mn, e = f - b * mn;
     int64_t i, j;
     if (mfast) {
       i = e % op.M;
@@ -36,6 +37,7 @@ __global__ void scale_kernel(Operands op, Scalars<T> s, int mfast) {
       i = e / op.N;
     }
     int64_t idx = op.Cbase + op.offMC[i] + op.offNC[j];
+    if (op.offBatch) idx += op.offBatch[2 * op.P + b];
     T v = s.beta_case == 0 ? tzero<T>() : cmul(load_c<T>(op.C, idx, op.TC), s.beta);
     store_c<T>(op.C, idx, op.TC, v);
   }
@@ -166,10 +168,18 @@ __device__ __forceinline__ void direct_gemm_tile(const Operands &op, const Scala
   }
 }
 
-template <class T, class Cfg>
+template <class T, class Cfg, bool BATCHED>
 __global__ void __launch_bounds__(256) direct_gemm_kernel(Operands op, Scalars<T> s, int a_mfast,
                                                           int b_nfast) {
-  direct_gemm_tile<T, Cfg>(op, s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+  if constexpr (!BATCHED) {
+    direct_gemm_tile<T, Cfg>(op, s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+    return;
+  }
+  // Batch labels: this tile of every batch entry z, z + gridDim.z, ...
+  for (int64_t b = blockIdx.z; b < op.P; b += gridDim.z) {
+    direct_gemm_tile<T, Cfg>(batch_entry(op, b), s, a_mfast, b_nfast, blockIdx.x, blockIdx.y);
+    __syncthreads();  // shared tiles are reused by the next entry
+  }
 }
 
 // Tile shapes: 0 = 64 x 64 (N > 32), 1 = 128 x 32 (16 < N <= 32),
@@ -239,9 +249,8 @@ __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJo
 constexpr int kSkinnyN = 16, kSkinnyK = 64;
 
 template <class T>
-__global__ void __launch_bounds__(256) skinny_kernel(Operands op, Scalars<T> s) {
-  __shared__ T Bs[kSkinnyK * kSkinnyN];
-  __shared__ int64_t sKA[kSkinnyK], sNC[kSkinnyN];
+__device__ __forceinline__ void skinny_entry(const Operands &op, const Scalars<T> &s, T *Bs, int64_t *sKA,
+                                             int64_t *sNC) {
   const int N = (int)op.N, K = (int)op.K;
   for (int e = threadIdx.x; e < K * N; e += blockDim.x) {
     const int k = e / N, j = e - k * N;
@@ -270,6 +279,21 @@ __global__ void __launch_bounds__(256) skinny_kernel(Operands op, Scalars<T> s) 
       const T old = s.beta_case == 0 ? tzero<T>() : load_c<T>(op.C, idx, op.TC);
       store_c<T>(op.C, idx, op.TC, axpby(s, acc[j], old));
     }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) skinny_kernel(Operands op, Scalars<T> s) {
+  __shared__ T Bs[kSkinnyK * kSkinnyN];
+  __shared__ int64_t sKA[kSkinnyK], sNC[kSkinnyN];
+  if (!op.offBatch) {
+    skinny_entry<T>(op, s, Bs, sKA, sNC);
+    return;
+  }
+  // Batch labels: entries y, y + gridDim.y, ... (B is staged per entry).
+  for (int64_t b = blockIdx.y; b < op.P; b += gridDim.y) {
+    skinny_entry<T>(batch_entry(op, b), s, Bs, sKA, sNC);
+    __syncthreads();  // before the next entry overwrites the staged B
   }
 }
 
@@ -409,7 +433,7 @@ template <class T>
 static cudaError_t launch_scale_t(const Operands &op, const double *alpha, const double *beta,
                                   int beta_case, int mfast, cudaStream_t st) {
   auto s = make_scalars<T>(alpha, beta, beta_case);
-  scale_kernel<T><<<grid_for(op.M * op.N, 256), 256, 0, st>>>(op, s, mfast);
+  scale_kernel<T><<<grid_for(op.M * op.N * op.P, 256), 256, 0, st>>>(op, s, mfast);
   return cudaGetLastError();
 }
 
@@ -428,8 +452,12 @@ template <class T, int SHAPE>
 static cudaError_t launch_direct_s(const Operands &op, const Scalars<T> &s, int a_mfast, int b_nfast,
                                    cudaStream_t st) {
   using Cfg = typename DirectShape<T, SHAPE>::Cfg;
-  dim3 grid((unsigned)((op.M + Cfg::BM - 1) / Cfg::BM), (unsigned)((op.N + Cfg::BN - 1) / Cfg::BN));
-  direct_gemm_kernel<T, Cfg><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
+  dim3 grid((unsigned)((op.M + Cfg::BM - 1) / Cfg::BM), (unsigned)((op.N + Cfg::BN - 1) / Cfg::BN),
+            (unsigned)(op.offBatch ? (op.P < 65535 ? op.P : 65535) : 1));
+  if (op.offBatch)
+    direct_gemm_kernel<T, Cfg, true><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
+  else
+    direct_gemm_kernel<T, Cfg, false><<<grid, 256, 0, st>>>(op, s, a_mfast, b_nfast);
   return cudaGetLastError();
 }
 
@@ -439,7 +467,9 @@ static cudaError_t launch_direct_t(int shape, const Operands &op, const double *
   auto s = make_scalars<T>(alpha, beta, beta_case);
   if (op.N <= kSkinnyN && op.K <= kSkinnyK) {
     const int64_t blocks = (op.M + 255) / 256;
-    skinny_kernel<T><<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(op, s);
+    dim3 grid((unsigned)(blocks < 148 * 16 ? blocks : 148 * 16),
+              (unsigned)(op.offBatch ? (op.P < 65535 ? op.P : 65535) : 1));
+    skinny_kernel<T><<<grid, 256, 0, st>>>(op, s);
     return cudaGetLastError();
   }
   switch (shape) {

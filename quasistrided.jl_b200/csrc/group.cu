@@ -276,6 +276,8 @@ int qs_group_create(int32_t n, qs_plan *const *plans, int32_t mode, qs_group **o
     if (!plans[i]) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
     if (plans[i]->host_only)
       return fail(QS_EINVAL, "ArgumentError: a host-only plan has no device workspace to execute");
+    if (plans[i]->batched)
+      return fail(QS_ENOTSUP, "ArgumentError: a plan with batch labels cannot join a group");
     for (int j = 0; j < i; ++j)
       if (plans[j] == plans[i]) return fail(QS_EINVAL, "ArgumentError: a plan appears twice in a group");
   }

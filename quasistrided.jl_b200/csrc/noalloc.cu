@@ -119,6 +119,8 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
   if (!alpha || !beta) return fail(QS_EINVAL, "ArgumentError: alpha/beta is NULL");
   qs_plan_options o{};
   if (opts) o = *opts;
+  if (o.flags & QS_PLAN_BATCH_LABELS)
+    return fail(QS_ENOTSUP, "ArgumentError: qs_contract_noalloc does not take batch labels");
   qs_plan p;  // host-side plan on the stack; no device workspace
   int rc = plan_host(&p, C, A, indA, B, indB, indC, &o);
   if (rc) return rc;

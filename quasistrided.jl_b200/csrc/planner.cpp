@@ -250,25 +250,32 @@ static bool free_unit_stride(const int64_t *labels, int D, const int64_t *ind, c
 // ----------------------------------------------------------------- plan ---
 
 int check_bounds(const qs_plan *p, bool reads_ab) {
-  auto span = [](int64_t base, const Group &g1, int p1, const Group &g2, int p2, int64_t len,
-                 const char *which) -> int {
-    int64_t rlo, rhi, clo, chi;
+  // bmap: which batch map adds to the range (0 = M-role operand, 1 = N-role
+  // operand, 2 = C); an unbatched plan's batch range is [0, 0].
+  auto span = [p](int64_t base, const Group &g1, int p1, const Group &g2, int p2, int bmap, int64_t len,
+                  const char *which) -> int {
+    int64_t rlo, rhi, clo, chi, blo = 0, bhi = 0;
     g1.offset_range(p1, rlo, rhi);
     g2.offset_range(p2, clo, chi);
     if (rhi < rlo || chi < clo) return QS_OK;
-    __int128 lo = (__int128)base + rlo + clo, hi = (__int128)base + rhi + chi;
+    if (p->batched) {
+      if (bmap == 2) p->bgc.offset_range(0, blo, bhi);
+      else p->bg.offset_range(bmap, blo, bhi);
+      if (bhi < blo) return QS_OK;
+    }
+    __int128 lo = (__int128)base + rlo + clo + blo, hi = (__int128)base + rhi + chi + bhi;
     if (lo >= 0 && hi <= (__int128)len - 1) return QS_OK;
     std::ostringstream s;
     s << "BoundsError: " << which << " addresses [" << (long long)lo << ", " << (long long)hi
       << "] exceed storage bounds [0, " << len - 1 << "]";
     return fail(QS_EBOUNDS, s.str());
   };
-  int rc = span(p->Cbase, p->mg, 1, p->ng, 1, p->Clen, "C");
+  int rc = span(p->Cbase, p->mg, 1, p->ng, 1, 2, p->Clen, "C");
   if (rc) return rc;
   if (reads_ab) {
-    rc = span(p->Abase, p->mg, 0, p->kg, 0, p->Alen, p->swapped ? "B" : "A");
+    rc = span(p->Abase, p->mg, 0, p->kg, 0, 0, p->Alen, p->swapped ? "B" : "A");
     if (rc) return rc;
-    rc = span(p->Bbase, p->ng, 0, p->kg, 1, p->Blen, p->swapped ? "A" : "B");
+    rc = span(p->Bbase, p->ng, 0, p->kg, 1, 1, p->Blen, p->swapped ? "A" : "B");
     if (rc) return rc;
   }
   return QS_OK;
@@ -356,11 +363,14 @@ int plan_host(qs_plan *p, const qs_view *C, const qs_view *A, const int64_t *ind
   if (!all_unique(indC, NC))
     return fail(QS_EINVAL, "ArgumentError: indC has a repeated label (diagonal), not supported: " +
                                tuple_str(indC, NC));
-  std::vector<int64_t> ml, nl, kl;
+  std::vector<int64_t> ml, nl, kl, bl;
+  const bool batch_ok = (o.flags & QS_PLAN_BATCH_LABELS) != 0;
   for (int i = 0; i < NA; ++i) {
     int64_t l = indA[i];
     bool inB = find_label(l, indB, NB) >= 0, inC = find_label(l, indC, NC) >= 0;
-    if (inB && inC) {
+    if (inB && inC && batch_ok) {
+      bl.push_back(l);
+    } else if (inB && inC) {
       std::ostringstream s;
       s << "ArgumentError: label " << l
         << " appears in indA, indB, and indC: labels present in all three operands "
@@ -399,7 +409,8 @@ int plan_host(qs_plan *p, const qs_view *C, const qs_view *A, const int64_t *ind
       return fail(QS_EINVAL, s.str());
     }
   }
-  if ((int)ml.size() > kMaxRank || (int)nl.size() > kMaxRank || (int)kl.size() > kMaxRank)
+  if ((int)ml.size() > kMaxRank || (int)nl.size() > kMaxRank || (int)kl.size() > kMaxRank ||
+      (int)bl.size() > kMaxRank)
     return fail(QS_EINVAL, "ArgumentError: more than 16 labels in one composite");
 
   // Free label order by |C stride| and C's unit-stride runs.
@@ -413,6 +424,9 @@ int plan_host(qs_plan *p, const qs_view *C, const qs_view *A, const int64_t *ind
   if ((rc = make_group(ng, nl.data(), (int)nl.size(), indB, B, indC, C))) return rc;
   // Validate K lengths in indA order first (DimensionMismatch before ordering).
   if ((rc = make_group(kg, kl.data(), (int)kl.size(), indA, A, indB, B))) return rc;
+  Group bg, bgc;
+  if ((rc = make_group(bg, bl.data(), (int)bl.size(), indA, A, indB, B))) return rc;
+  if ((rc = make_group(bgc, bl.data(), (int)bl.size(), indC, C, indA, A))) return rc;
 
   // K order: indA order, sorted by A's strides, sorted by B's strides;
   // ties keep indA order (src/planning/labels.jl:215-243).
@@ -491,6 +505,15 @@ int plan_host(qs_plan *p, const qs_view *C, const qs_view *A, const int64_t *ind
     p->kg = k2;
   }
   p->swapped = swap ? 1 : 0;
+  p->batched = bl.empty() ? 0 : 1;
+  p->bg = bg;
+  if (swap)
+    for (int d = 0; d < bg.D; ++d) {
+      p->bg.st[0][d] = bg.st[1][d];
+      p->bg.st[1][d] = bg.st[0][d];
+    }
+  p->bgc = bgc;
+  p->P = bg.length();
   p->M = p->mg.length();
   p->N = p->ng.length();
   p->K = p->kg.length();
@@ -523,11 +546,14 @@ int plan_host(qs_plan *p, const qs_view *C, const qs_view *A, const int64_t *ind
     }
   }
 
-  // select_path (src/planning/plan.jl:395-412), device thresholds.
-  if (p->M == 0 || p->N == 0) {
+  // select_path (src/planning/plan.jl:395-412), device thresholds.  A
+  // batched plan runs the gather GEMM (or a tensor-core method) per entry.
+  if (p->M == 0 || p->N == 0 || p->P == 0) {
     p->path = QS_PATH_EMPTY;
   } else if (p->K == 0) {
     p->path = QS_PATH_SCALE;
+  } else if (p->batched) {
+    p->path = QS_PATH_NEST;
   } else if ((p->M == 1 || p->N == 1) && p->K >= 32 && o.dot_mode != QS_MODE_NEVER) {
     p->path = QS_PATH_DOT;
   } else if (p->K == 1 && o.outer_mode != QS_MODE_NEVER) {

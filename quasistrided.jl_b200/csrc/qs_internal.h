@@ -65,6 +65,8 @@ struct Workspace {
   int64_t *offM[2] = {nullptr, nullptr};
   int64_t *offN[2] = {nullptr, nullptr};
   int64_t *offK[2] = {nullptr, nullptr};
+  // batch labels: [A offsets | B offsets | C offsets], P each, or nullptr
+  int64_t *offBatch = nullptr;
   // tensor-core paths: packed operand panels and per-row/col exponents
   void *panelA = nullptr;
   void *panelB = nullptr;
@@ -103,6 +105,12 @@ struct qs_plan {
   int64_t Abase = 0, Bbase = 0, Cbase = 0;
   qs::Group mg, ng, kg;
   int64_t M = 0, N = 0, K = 0;
+  // Batch labels (QS_PLAN_BATCH_LABELS): bg maps A and B (after the swap),
+  // bgc maps C; P batch entries; batch_host = the uploaded offset table.
+  int batched = 0;
+  qs::Group bg, bgc;
+  int64_t P = 1;
+  std::vector<int64_t> batch_host;
   int path = QS_PATH_EMPTY;
   int method = QS_METHOD_NATIVE;
   int complex_mode = QS_CPLX_NONE;
