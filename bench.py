@@ -177,8 +177,10 @@ def roofline(plan, stage_ms, nexec):
         ms = per.get("gemm_i8")
         peak = 2.0 * peaks["bf16_tflops"]
         note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
-        kernel = (f"oz_gemm_fixed_kernel<{s}, false>" if s in (6, 7) and not plan.per_product_gemm
-                  else "tc_gemm_kernel<KIND_I8>")
+        if s in (6, 7) and not plan.per_product_gemm:
+            kernel = f"oz_gemm_fixed_kernel<{s}, false>" if plan.oz_single_sm else f"oz_gemm_pair_kernel<{s}>"
+        else:
+            kernel = "tc_gemm_kernel<KIND_I8>"
     elif plan.method == "bf16x3":
         work = 3 * FLOPS
         ms = per.get("gemm_bf16")
@@ -247,7 +249,7 @@ def run_profile_target(args):
     Bv = qs.StridedView(torch.from_numpy(B_h).cuda(), sb, colmajor_strides(sb), 0)
     Cv = qs.StridedView(torch.from_numpy(C_h).cuda(), sc, colmajor_strides(sc), 0)
     plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method,
-                            per_product_gemm=args.per_product)
+                            per_product_gemm=args.per_product, oz_single_sm=args.oz_single_sm)
     qs.execute(plan, ALPHA, BETA)
     for _ in range(args.steps):
         qs.execute(plan, ALPHA, BETA)
@@ -696,6 +698,8 @@ def main():
     ap.add_argument("--method", default="auto", choices=["auto", "native", "ozaki"])
     ap.add_argument("--per-product", action="store_true",
                     help="Ozaki: the one-product-per-stage GEMM kernel instead of grouped diagonals")
+    ap.add_argument("--oz-single-sm", action="store_true",
+                    help="Ozaki: the one-SM GEMM kernel instead of the CTA-pair (cta_group::2) kernel")
     ap.add_argument("--cpu-rows", type=int, default=M)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
@@ -766,7 +770,7 @@ def main():
     Bv = qs.StridedView(Bd, sb, colmajor_strides(sb), 0)
     Cv = qs.StridedView(Cd, sc, colmajor_strides(sc), 0)
     plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method,
-                            per_product_gemm=args.per_product)
+                            per_product_gemm=args.per_product, oz_single_sm=args.oz_single_sm)
 
     # Accuracy of the measured path: one execution from the seeded C against
     # the FP64 oracle on a sample of C elements (first 2 rows of each 64-block

@@ -101,6 +101,8 @@ enum {
   QS_PLAN_CUDA_GRAPH = 4, /* qs_execute captures the plan's launches into a
                              CUDA graph once (again when alpha/beta change)
                              and replays it on later calls */
+  QS_PLAN_OZ_SINGLE_SM = 16, /* Ozaki with 6 or 7 slices: the one-SM GEMM kernel
+                                instead of the CTA-pair (cta_group::2) kernel */
   QS_PLAN_BATCH_LABELS = 8 /* accept labels present in A, B and C (which the
                               reference rejects, src/planning/labels.jl:48-54)
                               as batch labels: C[b,...] = alpha * sum_K

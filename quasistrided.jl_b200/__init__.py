@@ -212,6 +212,7 @@ class ContractPlan:
         self.workspace_bytes = info.workspace_bytes
         self.stride_class = info.stride_class
         self.native_tile = info.native_tile
+        self.oz_single_sm = False
         self.batch_labels = tuple(info.batch_labels[:info.batch_rank])
         self.batch_length = info.batch_length
 
@@ -261,7 +262,8 @@ class ContractPlan:
 def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=None,
              k_block=None, n_block=None, path_modes: Optional[PathModes] = None,
              ozaki_slices=0, complex_mode=None, host_only=False,
-             per_product_gemm=False, cuda_graph=False, batch_labels=False) -> _abi.qs_plan_options:
+             per_product_gemm=False, cuda_graph=False, batch_labels=False,
+             oz_single_sm=False) -> _abi.qs_plan_options:
     o = _abi.qs_plan_options()
     o.conjA, o.conjB = int(bool(conjA)), int(bool(conjB))
     o.accumulator = _acc_code(accumulator)
@@ -279,7 +281,8 @@ def _options(conjA=False, conjB=False, accumulator=None, method="auto", m_block=
     o.ozaki_slices = int(ozaki_slices)
     o.complex_mode = _abi.QS_CPLX[complex_mode]
     o.flags = ((_abi.QS_PLAN_HOST_ONLY if host_only else 0) | (2 if per_product_gemm else 0) |
-               (4 if cuda_graph else 0) | (_abi.QS_PLAN_BATCH_LABELS if batch_labels else 0))
+               (4 if cuda_graph else 0) | (_abi.QS_PLAN_BATCH_LABELS if batch_labels else 0) |
+               (_abi.QS_PLAN_OZ_SINGLE_SM if oz_single_sm else 0))
     return o
 
 
@@ -305,14 +308,16 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                   n_block=None, allocator=None, accumulator=None,
                   path_modes: Optional[PathModes] = None, method="auto", ozaki_slices=0,
                   complex_mode=None, host_only=False, per_product_gemm=False,
-                  cuda_graph=False, native_tile=0, batch_labels=False) -> ContractPlan:
+                  cuda_graph=False, native_tile=0, batch_labels=False,
+                  oz_single_sm=False) -> ContractPlan:
     """Plan ``C[indC] = A[indA] * B[indB]`` (every label in exactly two operands).
 
     Throws ArgumentError / DimensionMismatch on invalid input, before any
     device work.  ``kernel`` names a method ("native", "ozaki", "bf16x3");
     ``cuda_graph`` makes ``execute`` replay a captured CUDA graph of the
     plan's launches (re-captured when alpha/beta change);
-    ``batch_labels=True`` accepts labels present in A, B and C (the
+    ``oz_single_sm=True`` runs the Ozaki GEMM (6 or 7 slices) on the one-SM
+    kernel instead of the CTA-pair kernel.  ``batch_labels=True`` accepts labels present in A, B and C (the
     reference rejects them) as batch labels: one contraction per batch entry.
     ``allocator`` serves the plan's device workspace (None: the library's
     pool; a ``DeviceArena`` or ``TorchAllocator``), handed back in reverse
@@ -328,7 +333,8 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
     iB = _labels(indB, B.ndim, "indB", keep)
     iC = _labels(indC, C.ndim, "indC", keep)
     o = _options(conjA, conjB, accumulator, method, m_block, k_block, n_block, path_modes,
-                 ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph, batch_labels)
+                 ozaki_slices, complex_mode, host_only, per_product_gemm, cuda_graph, batch_labels,
+                 oz_single_sm)
     o.native_tile = int(native_tile)
     o.allocator = None if host_only else allocator_handle(allocator)
     h = ctypes.c_void_p()
@@ -336,6 +342,7 @@ def plan_contract(C: StridedView, A: StridedView, indA, B: StridedView, indB, in
                                            ctypes.byref(cB), iB, iC, ctypes.byref(o)))
     plan = ContractPlan(h, C, A, B, host_only)
     plan.per_product_gemm, plan.cuda_graph = bool(per_product_gemm), bool(cuda_graph)
+    plan.oz_single_sm = bool(oz_single_sm)
     plan.allocator = allocator
     return plan
 

@@ -18,6 +18,7 @@ QS_PATH_NAME = {0: "EmptyPath", 1: "ScalePath", 2: "DotPath", 3: "OuterPath", 4:
 QS_CPLX = {None: 0, "planar": 1, "1m": 2}
 QS_PLAN_HOST_ONLY = 1
 QS_PLAN_BATCH_LABELS = 8
+QS_PLAN_OZ_SINGLE_SM = 16
 
 ELTYPE_NAME = {QS_F32: "Float32", QS_F64: "Float64", QS_C32: "ComplexF32", QS_C64: "ComplexF64"}
 

@@ -1,6 +1,8 @@
 // Inline-PTX wrappers for sm_100a: mbarriers with bounded waits, bulk
 // global->shared copies, and the tcgen05 family (TMEM allocation, MMA,
-// commit, loads/stores).  Written from the PTX ISA; no multicast anywhere.
+// commit, loads/stores).  Written from the PTX ISA.  No load multicasts: the
+// one multicast is tc_commit_pair's mbarrier arrive to the two CTAs of a
+// pair, which moves no data.
 #pragma once
 
 #include <cstdint>
@@ -124,6 +126,84 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
+}
+
+// ------------------------------------------- CTA pairs (cta_group::2) ----
+// A cluster of two CTAs on two SMs sharing one MMA: the even CTA issues
+// tcgen05.mma.cta_group::2 over both CTAs' shared memory (each holds half of
+// A's rows and half of B's columns) into both CTAs' TMEM (each its own rows).
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Every thread of both CTAs; orders shared-memory and barrier state.
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+// Arrive on the mbarrier at the same shared-memory offset in CTA `cta`
+// (default semantics, no cluster-scope fence on the critical path).
+__device__ __forceinline__ void mbar_arrive_cluster(uint64_t *bar, uint32_t cta) {
+  asm volatile(
+      "{\n\t.reg .b32 ra;\n\t"
+      "mapa.shared::cluster.u32 ra, %0, %1;\n\t"
+      "mbarrier.arrive.shared::cluster.b64 _, [ra];\n\t}" ::"r"(smem_u32(bar)),
+      "r"(cta)
+      : "memory");
+}
+// Arrive on `bar` in both CTAs of the pair once this thread's tcgen05
+// operations complete.
+__device__ __forceinline__ void tc_commit_pair(uint64_t *bar) {
+  asm volatile(
+      "{\n\t.reg .b16 m;\n\t"
+      "mov.b16 m, 3;\n\t"
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m;\n\t}" ::
+          "r"(smem_u32(bar))
+      : "memory");
+}
+// D[tmem of both CTAs] (+)= A[smem of both] * B[smem of both]^T, int8 -> int32;
+// M = 256 (128 rows per CTA), N split 50/50 between the CTAs' B tiles.
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// Shared::cluster address of the object at `p`'s offset in CTA `cta`.
+__device__ __forceinline__ uint32_t mapa_u32(const void *p, uint32_t cta) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(cta));
+  return r;
+}
+// Tiled 2-D tensor load (no multicast) into this CTA's shared memory whose
+// byte count completes on the mbarrier at shared::cluster address `mbar`,
+// which may be the other CTA's of the pair (cta_group::2).  x is 0 here.
+__device__ __forceinline__ void tma_load_2d_pair(void *smem_dst, const void *tmap, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(mbar), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Issued by the same warp of both CTAs, with the same shared-memory slot.
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t *smem_dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(smem_dst)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
 }
 
 // 32 lanes x 16 consecutive 32-bit columns (one register per column).

@@ -139,6 +139,10 @@ struct qs_plan {
   int native_shape = 0;  // gather-GEMM tile shape (direct_shape numbering)
   qs::TensorCoreGeom tc;
   qs::Workspace ws;
+  // CTA-pair Ozaki kernel: tensor maps (CUtensorMap bytes) of the A and B
+  // panels, made once the panels exist; oz_pair_maps == 0 -> one-SM kernel.
+  int oz_pair_maps = 0;
+  unsigned char oz_tmap[256] = {};
   // Instrumentation (qs_plan_profile): cudaEvent_t handles, kProfStages+1
   // per recorded execute.
   static constexpr int kProfExec = 256, kProfStages = 5;

@@ -16,8 +16,10 @@
 // conjugation on load, and writes K-major panels in the exact byte image of
 // the 128-byte-swizzled shared-memory tiles the MMA reads, so the GEMM moves
 // whole tiles with single bulk copies.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <climits>
 #include <cmath>
@@ -1092,6 +1094,7 @@ __device__ __forceinline__ void oz_slot(uint32_t s0, uint32_t par0, int l, uint3
 }
 
 #include "oz_fixed.cuh"
+#include "oz_2sm.cuh"
 
 // The group schedule of the v2 kernel for s slices (host).
 static OzSched build_oz_sched(int s) {
@@ -1261,9 +1264,13 @@ void tc_geometry(qs_plan *p) {
     g.kblocks = cdiv(Kv, 128);
     g.mtiles = cdiv(Mv, 128);
     g.ntiles = cdiv(Nv, 128);
-    g.Mp = g.mtiles * 128;
+    // The CTA-pair kernel (6 or 7 slices) reads M tiles in pairs: the A
+    // panel holds an even number of them (a padding tile's rows are never
+    // stored, and rows of A do not mix).
+    const int64_t mt_alloc = (g.nslices == 6 || g.nslices == 7) ? (g.mtiles + 1) / 2 * 2 : g.mtiles;
+    g.Mp = mt_alloc * 128;
     g.Np = g.ntiles * 128;
-    g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
+    g.plane_bytes_a = mt_alloc * g.kblocks * 128 * 128;
     g.plane_bytes_b = g.ntiles * g.kblocks * 128 * 128;
     // INT32-exact segment: (terms) * kblocks * 128 * 127^2 < 2^31.
     int64_t maxkb = (int64_t)(2147483647ll / ((int64_t)g.nslices * 128 * 127 * 127));
@@ -1284,6 +1291,49 @@ void tc_geometry(qs_plan *p) {
 
 static int tc_alloc(qs_plan *p, void **out, size_t bytes) { return plan_alloc(p, out, bytes); }
 
+// Tensor maps of the packed Ozaki panels for the CTA-pair kernel: each panel
+// as a 2-D array of 128-byte rows (slices x tiles x K blocks x 128 rows),
+// copied unswizzled (the tiles are stored swizzled); boxes of 128 rows for A
+// and 64 rows (one CTA's half of a B tile) for B.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+static bool encode_panel_map(CUtensorMap *m, void *base, uint64_t rows, uint32_t box_rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc || rows == 0 || rows > 0x7fffffffull || (reinterpret_cast<uintptr_t>(base) & 15)) return false;
+  const cuuint64_t dims[2] = {128, rows};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {128, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static bool make_pair_maps(qs_plan *p) {
+  static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
+  const TensorCoreGeom &g = p->tc;
+  CUtensorMap ma, mb;
+  if (!encode_panel_map(&ma, p->ws.panelA, (uint64_t)g.plane_bytes_a * g.nslices / 128, 128) ||
+      !encode_panel_map(&mb, p->ws.panelB, (uint64_t)g.plane_bytes_b * g.nslices / 128, 64))
+    return false;
+  std::memcpy(p->oz_tmap, &ma, 128);
+  std::memcpy(p->oz_tmap + 128, &mb, 128);
+  return true;
+}
+
 int tc_prepare(qs_plan *p) {
   tc_geometry(p);
   const TensorCoreGeom &g = p->tc;
@@ -1293,6 +1343,9 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelA = q;
   if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_b * g.nslices))) return rc;
   p->ws.panelB = q;
+  if (p->method == QS_METHOD_OZAKI_I8 && (g.nslices == 6 || g.nslices == 7) &&
+      !(p->opts.flags & (QS_PLAN_OZ_SINGLE_SM | QS_PLAN_PER_PRODUCT_GEMM)))
+    p->oz_pair_maps = make_pair_maps(p) ? 1 : 0;  // else the one-SM kernel runs
   if (p->method == QS_METHOD_OZAKI_I8) {
     // exponents (padded rows/cols), non-finite lists, their counters, status
     size_t n = (size_t)(g.Mp + g.Np + g.Mp + g.Np + 4);
@@ -1325,6 +1378,10 @@ int tc_prepare(qs_plan *p) {
     cudaFuncSetAttribute(oz_gemm_fixed_kernel<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_fixed_kernel<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_pair_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_pair_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     attr_set[0] = attr_set[1] = true;
   }
@@ -1440,6 +1497,43 @@ static FixupJob make_fixup_job(const qs_plan *p, const double *alpha, const doub
   return f;
 }
 
+// The CTA-pair Ozaki GEMM: clusters of two CTAs, as many as fit at once
+// (persistent), each pair looping over 256 x 128 tiles of C.
+static cudaError_t launch_oz_pair(int S, const GemmArgs &a, const unsigned char *maps, cudaStream_t st) {
+  CUtensorMap ma, mb;
+  std::memcpy(&ma, maps, 128);
+  std::memcpy(&mb, maps + 128, 128);
+  static int max_clusters[2] = {0, 0};
+  const int si = S == 6 ? 0 : 1;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(320, 1, 1);
+  cfg.dynamicSmemBytes = oz_smem_bytes();
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (!max_clusters[si]) {
+    cfg.gridDim = dim3(2 * (unsigned)(num_sms() / 2), 1, 1);
+    int n = 0;
+    cudaError_t e = S == 6 ? cudaOccupancyMaxActiveClusters(&n, oz_gemm_pair_kernel<6>, &cfg)
+                           : cudaOccupancyMaxActiveClusters(&n, oz_gemm_pair_kernel<7>, &cfg);
+    if (e != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+    }
+    max_clusters[si] = n;
+  }
+  const int pairs = (a.mtiles + 1) / 2 * a.ntiles;
+  const int clusters = std::min(pairs, max_clusters[si]);
+  cfg.gridDim = dim3(2 * (unsigned)clusters, 1, 1);
+  return S == 6 ? cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<6>, a, ma, mb)
+                : cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<7>, a, ma, mb);
+}
+
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
                cudaStream_t st, cudaEvent_t *ev) {
   const TensorCoreGeom &g = p->tc;
@@ -1477,6 +1571,9 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   if (oz) {
     if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) {
       tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+    } else if ((g.nslices == 6 || g.nslices == 7) && p->oz_pair_maps) {
+      e = launch_oz_pair(g.nslices, a, p->oz_tmap, st);
+      if (e != cudaSuccess) return fail(QS_ECUDA, std::string("CTA-pair GEMM launch: ") + cudaGetErrorString(e));
     } else if (g.nslices == 6) {
       oz_gemm_fixed_kernel<6, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices == 7) {
