@@ -266,15 +266,51 @@ __device__ __forceinline__ void bf16_pack_block(const PackArgs &a, int64_t r0, i
   *reinterpret_cast<uint4 *>(a.panel + a.plane + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 
-// One plan: grid (row blocks of 32, K blocks).
-__global__ void __launch_bounds__(256) oz_rowmax_kernel(PackArgs a, unsigned long long *rowmax) {
-  oz_rowmax_block(a, rowmax, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 128);
+// Both operands of one plan in one launch (A's and B's packs are
+// independent): blocks [0, nA) take A's (row block, K block) pairs, row block
+// fastest, the rest B's.  Twice the blocks in flight and half the launch
+// tails of one launch per operand.
+__device__ __forceinline__ void split_block(int64_t b, int nrb, int64_t &r0, int64_t &kb) {
+  r0 = (b % nrb) * 32;
+  kb = b / nrb;
 }
-__global__ void __launch_bounds__(256) oz_slice_kernel(PackArgs a, const unsigned long long *rowmax) {
-  oz_slice_block(a, rowmax, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 128);
+__global__ void __launch_bounds__(256, 6)  // six 33 KB tiles per SM, as one operand per launch had
+    oz_rowmax_pair_kernel(PackArgs pa, PackArgs pb, unsigned long long *rma, unsigned long long *rmb, int nrbA,
+                          int nrbB, int64_t nA) {
+  int64_t r0, kb;
+  const int64_t b = blockIdx.x;
+  if (b < nA) {
+    split_block(b, nrbA, r0, kb);
+    oz_rowmax_block(pa, rma, r0, kb * 128);
+  } else {
+    split_block(b - nA, nrbB, r0, kb);
+    oz_rowmax_block(pb, rmb, r0, kb * 128);
+  }
 }
-__global__ void __launch_bounds__(256) bf16_pack_kernel(PackArgs a) {
-  bf16_pack_block(a, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 64);
+__global__ void __launch_bounds__(256)
+    oz_slice_pair_kernel(PackArgs pa, PackArgs pb, const unsigned long long *rma, const unsigned long long *rmb,
+                         int nrbA, int nrbB, int64_t nA) {
+  int64_t r0, kb;
+  const int64_t b = blockIdx.x;
+  if (b < nA) {
+    split_block(b, nrbA, r0, kb);
+    oz_slice_block(pa, rma, r0, kb * 128);
+  } else {
+    split_block(b - nA, nrbB, r0, kb);
+    oz_slice_block(pb, rmb, r0, kb * 128);
+  }
+}
+__global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackArgs pb, int nrbA, int nrbB,
+                                                             int64_t nA) {
+  int64_t r0, kb;
+  const int64_t b = blockIdx.x;
+  if (b < nA) {
+    split_block(b, nrbA, r0, kb);
+    bf16_pack_block(pa, r0, kb * 64);
+  } else {
+    split_block(b - nA, nrbB, r0, kb);
+    bf16_pack_block(pb, r0, kb * 64);
+  }
 }
 
 // ---------------------------------------------------------------- GEMM ---
@@ -1550,20 +1586,27 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     e = cudaMemsetAsync(p->ws.rowmax, 0, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
-  for (int side = 0; side < 2; ++side) {
-    PackArgs pa = pack_args(p, side);
+  {
+    // Both operands per launch.  Profile stages: Ozaki ev[1] after the
+    // row-max pass, ev[2] after the digit planes; BF16x3 both after the pack.
+    const PackArgs pa = pack_args(p, 0), pb = pack_args(p, 1);
+    const int nrbA = (int)cdiv(pa.rows_pad, 32), nrbB = (int)cdiv(pb.rows_pad, 32);
+    const int64_t nA = (int64_t)nrbA * g.kblocks, nB = (int64_t)nrbB * g.kblocks;
     if (oz) {
-      unsigned long long *rm = (unsigned long long *)p->ws.rowmax + (side ? g.Mp : 0);
-      dim3 grid((unsigned)cdiv(pa.rows_pad, 32), (unsigned)g.kblocks);
-      oz_rowmax_kernel<<<grid, 256, 0, st>>>(pa, rm);
-      oz_slice_kernel<<<grid, 256, 0, st>>>(pa, rm);
+      unsigned long long *rma = (unsigned long long *)p->ws.rowmax, *rmb = rma + g.Mp;
+      oz_rowmax_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, rma, rmb, nrbA, nrbB, nA);
+      if (ev) cudaEventRecord(ev[1], st);
+      oz_slice_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, rma, rmb, nrbA, nrbB, nA);
+      if (ev) cudaEventRecord(ev[2], st);
       launches += 2;
     } else {
-      dim3 grid((unsigned)cdiv(pa.rows_pad, 32), (unsigned)g.kblocks);
-      bf16_pack_kernel<<<grid, 256, 0, st>>>(pa);
+      bf16_pack_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, nrbA, nrbB, nA);
+      if (ev) {
+        cudaEventRecord(ev[1], st);
+        cudaEventRecord(ev[2], st);
+      }
       ++launches;
     }
-    if (ev) cudaEventRecord(ev[side + 1], st);
   }
   const GemmArgs a = make_gemm_args(p, alpha, beta, beta_case);
   const int tiles = a.mtiles * a.ntiles;
