@@ -13,6 +13,10 @@
  *     src/integrations/tensoroperations.jl:299-307
  *   TO.tensorcontract! label mapping              -> qs_contraction_labels
  *     src/integrations/tensoroperations.jl:315-322
+ *   TO.tensoradd! / TO.tensortrace! (forwarded to StridedNative there)
+ *     src/integrations/tensoroperations.jl:91-107  -> qs_tensoradd_trace
+ *   TensorOperations allocators for the workspace -> qs_plan_options.allocator,
+ *     src/execution/workspace.jl:98-123              qs_arena_* (BufferAllocator)
  *
  * Conventions
  *  - Every operand is a qs_view: a parent allocation (`data`, `length`
