@@ -179,7 +179,7 @@ def roofline(plan, stage_ms, nexec):
         ms = per.get("gemm_i8")
         peak = 2.0 * peaks["bf16_tflops"]
         note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
-        if s in (6, 7) and not plan.per_product_gemm:
+        if s in (4, 6, 7) and not plan.per_product_gemm:
             kernel = f"oz_gemm_fixed_kernel<{s}, false>" if plan.oz_single_sm else f"oz_gemm_pair_kernel<{s}>"
         else:
             kernel = "tc_gemm_kernel<KIND_I8>"
@@ -777,7 +777,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--method", default="auto", choices=["auto", "native", "ozaki"])
+    ap.add_argument("--method", default="auto", choices=["auto", "native", "ozaki", "bf16x3"])
+    ap.add_argument("--dist", default="uniform", choices=["uniform", "wide"],
+                    help="c1 inputs: uniform[-1,1], or that times 2^U (U in [-20,20]) per a-slice of A and "
+                         "per d-slice of B")
+    ap.add_argument("--c1-dtype", default="f64", choices=["f64", "f32"],
+                    help="c1 element type (f32 runs the split-BF16x3 tensor-core method by default)")
     ap.add_argument("--per-product", action="store_true",
                     help="Ozaki: the one-product-per-stage GEMM kernel instead of grouped diagonals")
     ap.add_argument("--oz-single-sm", action="store_true",
@@ -845,7 +850,12 @@ def main():
     qs = load_engine()
     dev = torch.device("cuda", local)
 
-    A_h, B_h, C_h = host_inputs(seed=20261203 + rank)
+    A_h, B_h, C_h = host_inputs(seed=20261203 + rank, wide=args.dist == "wide")
+    f32 = args.c1_dtype == "f32"
+    if f32:
+        # Float32 operands; the accuracy reference is FP64 on the same values.
+        A_h, B_h, C_h = (x.astype(np.float32) for x in (A_h, B_h, C_h))
+    esize = A_h.itemsize
     sa, sb, sc = shapes()
     Ad = torch.from_numpy(A_h).to(dev)
     Bd = torch.from_numpy(B_h).to(dev)
@@ -865,12 +875,12 @@ def main():
     torch.cuda.synchronize()
     got = Cd.cpu().numpy()
     nsamp = 8192
-    Cref = orc.HostView(C_h.copy(), sc, colmajor_strides(sc))
-    orc.brute(Cref, ALPHA, orc.HostView(A_h, sa, colmajor_strides(sa)), LABELS["indA"],
-              orc.HostView(B_h, sb, colmajor_strides(sb)), LABELS["indB"], BETA, LABELS["indC"],
+    Cref = orc.HostView(C_h.astype(np.float64), sc, colmajor_strides(sc))
+    orc.brute(Cref, ALPHA, orc.HostView(A_h.astype(np.float64), sa, colmajor_strides(sa)), LABELS["indA"],
+              orc.HostView(B_h.astype(np.float64), sb, colmajor_strides(sb)), LABELS["indB"], BETA, LABELS["indC"],
               c_range=(0, nsamp))
     ref = Cref.parent[:nsamp]
-    rel_err = float(np.linalg.norm(got[:nsamp] - ref) / np.linalg.norm(ref))
+    rel_err = float(np.linalg.norm(got[:nsamp].astype(np.float64) - ref) / np.linalg.norm(ref))
 
     stream = torch.cuda.current_stream()
     # warm-up (untimed)
@@ -917,12 +927,13 @@ def main():
     B_p = torch.from_numpy(B_h).pin_memory()
     C_p = torch.from_numpy(C_h).pin_memory()
     outs = [torch.empty_like(C_p).pin_memory() for _ in range(2)]
-    h2d = (A_p.numel() + B_p.numel() + C_p.numel()) * 8
-    d2h = outs[0].numel() * 8
+    h2d = (A_p.numel() + B_p.numel() + C_p.numel()) * esize
+    d2h = outs[0].numel() * esize
     A1d, B1d, C1d = torch.empty_like(Ad), torch.empty_like(Bd), torch.empty_like(Cd)
     plan1 = qs.plan_contract(qs.StridedView(C1d, sc, colmajor_strides(sc), 0), qs.StridedView(A1d, sa, colmajor_strides(sa), 0),
                              LABELS["indA"], qs.StridedView(B1d, sb, colmajor_strides(sb), 0), LABELS["indB"],
-                             LABELS["indC"], method=args.method, per_product_gemm=args.per_product)
+                             LABELS["indC"], method=args.method, per_product_gemm=args.per_product,
+                             oz_single_sm=args.oz_single_sm)
     bufs = [(Ad, Bd, Cd, plan), (A1d, B1d, C1d, plan1)]
     s_in, s_run, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
     ev_in = [torch.cuda.Event() for _ in range(2)]
@@ -962,7 +973,7 @@ def main():
     plan1.release()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not f32:
         # Passes over args.cpu_rows rows of M until at least args.cpu_seconds
         # of CPU work (at most 16 passes); the median rate is reported.
         rates, total = [], 0.0
@@ -976,13 +987,19 @@ def main():
 
     if rank == 0:
         print(json.dumps({
-            "metric": "contraction TFLOP/s (Float64, rel.err<=1e-13 vs FP64)",
+            "metric": ("contraction TFLOP/s (Float32, rel.err<=1e-5 vs FP64)" if f32 else
+                       "contraction TFLOP/s (Float64, rel.err<=1e-13 vs FP64)"),
             "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1] A/B, N(0,1) C)",
+            "vs_baseline": None, "dtype": args.c1_dtype,
+            "data": ("synthetic (seeded uniform[-1,1] A/B" +
+                     (" x 2^U per a-slice of A and d-slice of B, U in [-20,20]" if args.dist == "wide" else "") +
+                     ", N(0,1) C)"),
             "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "alpha": ALPHA, "beta": BETA,
                        "method": plan.method, "ozaki_slices": plan.ozaki_slices,
-                       "l2": "inputs larger than L2 (419 MB), no flush", "parallelism": f"replicas{world}"},
+                       "dist": args.dist,
+                       "l2": f"inputs larger than L2 ({419 if not f32 else 210} MB), no flush",
+                       "parallelism": f"replicas{world}"},
             "rel_err": rel_err, "rel_err_sample": nsamp,
             "roofline": roof, "stages_ms": stages,
             "cpu_baseline": cpu,

@@ -3,8 +3,8 @@
 For a contraction it picks the plan options that run fastest on this GPU
 while meeting the accuracy target:
 
-* method: the gather GEMM (``native``) or the tensor-core path (``ozaki`` for
-  Float64/ComplexF64, ``bf16x3`` for Float32/ComplexF32);
+* method: the gather GEMM (``native``) or a tensor-core path (``ozaki`` for
+  every compute type, ``bf16x3`` also for Float32/ComplexF32);
 * the Ozaki GEMM kernel (grouped diagonals, or one product per stage);
 * the gather GEMM's tile shape (64x64, 128x32, 256x16, 32x32; real types);
 * the Ozaki slice count: the default for K, raised while a probe on random
@@ -101,8 +101,8 @@ class Autotuner:
             out += [{"method": "native", "native_tile": t} for t in (1, 2, 3, 4)]
         else:
             out.append({"method": "native"})
+        out.append({"method": "ozaki"})
         if dbl:
-            out.append({"method": "ozaki"})
             out.append({"method": "ozaki", "per_product_gemm": True})
         else:
             out.append({"method": "bf16x3"})

@@ -308,8 +308,6 @@ int upload_offsets(qs_plan *p) {
 int choose_method(qs_plan *p) {
   int want = p->opts.method;
   bool dbl = is_double(p->T);
-  if (want == QS_METHOD_OZAKI_I8 && !dbl)
-    return fail(QS_ENOTSUP, "ArgumentError: the Ozaki INT8 method needs a Float64/ComplexF64 compute type");
   if (want == QS_METHOD_BF16X3 && dbl)
     return fail(QS_ENOTSUP, "ArgumentError: the split-BF16x3 method needs a Float32/ComplexF32 compute type");
   if (want < QS_METHOD_AUTO || want > QS_METHOD_BF16X3)

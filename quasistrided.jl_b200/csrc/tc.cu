@@ -1257,16 +1257,26 @@ int tc_auto_method(const qs_plan *p) {
   const int64_t n = is_complex(p->T) ? 2 * p->N : p->N;
   if (m < 128 || n < 64 || p->K < 64) return QS_METHOD_NATIVE;
   if ((double)p->M * (double)p->N * (double)p->K < 67108864.0) return QS_METHOD_NATIVE;
-  return is_double(p->T) ? QS_METHOD_OZAKI_I8 : QS_METHOD_BF16X3;
+  // Single precision too: 4 INT8 digits (10 products) stay within 1e-5 of
+  // FP64 (about 1e-9 before the final rounding), where split BF16x3 keeps
+  // about 16 mantissa bits (~1e-5 relative error on its own); BF16x3 stays
+  // available by request.
+  return QS_METHOD_OZAKI_I8;
 }
 
-static int default_slices(int64_t K, bool cplx) {
+// Slice counts with a compile-time (fixed-schedule) GEMM kernel.
+static bool oz_fixed_slices(int s) { return s == 4 || s == 6 || s == 7; }
+
+static int default_slices(int64_t K, bool cplx, bool dbl) {
   // The relative error of s base-254 digits is about 254^-s times
   // (row max / row rms of A + column max / column rms of B): ~1e-14 for
   // s = 6 on uniform inputs at K = 2304 (max/rms = sqrt 3), but up to ~1e-13
   // for Gaussian rows of a few thousand elements (max/rms ~ 4), which the
   // 1m form of complex data (K doubled) reaches.  7 digits (28 products)
   // for complex compute types and for K beyond 4096, else 6 (21 products).
+  // Single precision (24 significand bits) needs 4 digits: ~1e-9 relative
+  // before the one rounding to Float32.
+  if (!dbl) return 4;
   int s = 6;
   if (cplx || K > 4096) s = 7;
   return s;
@@ -1295,7 +1305,7 @@ void tc_geometry(qs_plan *p) {
   const int64_t Mv = p->M * g.rows_per_elem_a, Nv = p->N * g.cols_per_elem_b;
   const int64_t Kv = cx ? 2 * p->K : p->K;
   if (p->method == QS_METHOD_OZAKI_I8) {
-    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv, cx);
+    g.nslices = p->opts.ozaki_slices > 0 ? p->opts.ozaki_slices : default_slices(Kv, cx, is_double(p->T));
     p->ozaki_slices = g.nslices;
     g.kblocks = cdiv(Kv, 128);
     g.mtiles = cdiv(Mv, 128);
@@ -1303,7 +1313,7 @@ void tc_geometry(qs_plan *p) {
     // The CTA-pair kernel (6 or 7 slices) reads M tiles in pairs: the A
     // panel holds an even number of them (a padding tile's rows are never
     // stored, and rows of A do not mix).
-    const int64_t mt_alloc = (g.nslices == 6 || g.nslices == 7) ? (g.mtiles + 1) / 2 * 2 : g.mtiles;
+    const int64_t mt_alloc = oz_fixed_slices(g.nslices) ? (g.mtiles + 1) / 2 * 2 : g.mtiles;
     g.Mp = mt_alloc * 128;
     g.Np = g.ntiles * 128;
     g.plane_bytes_a = mt_alloc * g.kblocks * 128 * 128;
@@ -1379,7 +1389,7 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelA = q;
   if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_b * g.nslices))) return rc;
   p->ws.panelB = q;
-  if (p->method == QS_METHOD_OZAKI_I8 && (g.nslices == 6 || g.nslices == 7) &&
+  if (p->method == QS_METHOD_OZAKI_I8 && oz_fixed_slices(g.nslices) &&
       !(p->opts.flags & (QS_PLAN_OZ_SINGLE_SM | QS_PLAN_PER_PRODUCT_GEMM)))
     p->oz_pair_maps = make_pair_maps(p) ? 1 : 0;  // else the one-SM kernel runs
   if (p->method == QS_METHOD_OZAKI_I8) {
@@ -1414,6 +1424,10 @@ int tc_prepare(qs_plan *p) {
     cudaFuncSetAttribute(oz_gemm_fixed_kernel<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_fixed_kernel<7, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_pair_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
@@ -1496,10 +1510,13 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.M = p->M * g.rows_per_elem_a;
   a.N = p->N * g.cols_per_elem_b;
   a.cplx = g.cplx_layout;
-  a.alpha_im = alpha[1];
-  a.beta_im = beta[1];
-  a.alpha = alpha[0];
-  a.beta = beta[0];
+  // alpha/beta converted to the compute type first (convert(T, alpha)); the
+  // Ozaki epilogue then works in FP64 and rounds once to eltype(C).
+  auto cv = [p](double x) { return is_double(p->T) ? x : (double)(float)x; };
+  a.alpha_im = cv(alpha[1]);
+  a.beta_im = cv(beta[1]);
+  a.alpha = cv(alpha[0]);
+  a.beta = cv(beta[0]);
   a.beta_case = beta_case;
   a.status = p->ws.status;
   for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
@@ -1519,8 +1536,9 @@ static FixupJob make_fixup_job(const qs_plan *p, const double *alpha, const doub
   op.offNB = p->ws.offN[0]; op.offNC = p->ws.offN[1];
   op.offKA = p->ws.offK[0]; op.offKB = p->ws.offK[1];
   op.M = p->M; op.N = p->N; op.K = p->K;
-  f.alpha[0] = alpha[0]; f.alpha[1] = alpha[1];
-  f.beta[0] = beta[0]; f.beta[1] = beta[1];
+  auto cv = [p](double x) { return is_double(p->T) ? x : (double)(float)x; };
+  f.alpha[0] = cv(alpha[0]); f.alpha[1] = cv(alpha[1]);
+  f.beta[0] = cv(beta[0]); f.beta[1] = cv(beta[1]);
   f.beta_case = beta_case;
   f.cplx = g.cplx_layout;
   int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
@@ -1539,8 +1557,10 @@ static cudaError_t launch_oz_pair(int S, const GemmArgs &a, const unsigned char 
   CUtensorMap ma, mb;
   std::memcpy(&ma, maps, 128);
   std::memcpy(&mb, maps + 128, 128);
-  static int max_clusters[2] = {0, 0};
-  const int si = S == 6 ? 0 : 1;
+  static int max_clusters[3] = {0, 0, 0};
+  const int si = S == 4 ? 0 : S == 6 ? 1 : 2;
+  const void *kern = S == 4 ? (const void *)oz_gemm_pair_kernel<4>
+                   : S == 6 ? (const void *)oz_gemm_pair_kernel<6> : (const void *)oz_gemm_pair_kernel<7>;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1555,8 +1575,7 @@ static cudaError_t launch_oz_pair(int S, const GemmArgs &a, const unsigned char 
   if (!max_clusters[si]) {
     cfg.gridDim = dim3(2 * (unsigned)(num_sms() / 2), 1, 1);
     int n = 0;
-    cudaError_t e = S == 6 ? cudaOccupancyMaxActiveClusters(&n, oz_gemm_pair_kernel<6>, &cfg)
-                           : cudaOccupancyMaxActiveClusters(&n, oz_gemm_pair_kernel<7>, &cfg);
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
     if (e != cudaSuccess || n < 1) {
       cudaGetLastError();
       return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
@@ -1566,8 +1585,9 @@ static cudaError_t launch_oz_pair(int S, const GemmArgs &a, const unsigned char 
   const int pairs = (a.mtiles + 1) / 2 * a.ntiles;
   const int clusters = std::min(pairs, max_clusters[si]);
   cfg.gridDim = dim3(2 * (unsigned)clusters, 1, 1);
-  return S == 6 ? cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<6>, a, ma, mb)
-                : cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<7>, a, ma, mb);
+  if (S == 4) return cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<4>, a, ma, mb);
+  if (S == 6) return cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<6>, a, ma, mb);
+  return cudaLaunchKernelEx(&cfg, oz_gemm_pair_kernel<7>, a, ma, mb);
 }
 
 int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_case,
@@ -1614,9 +1634,11 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   if (oz) {
     if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) {
       tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
-    } else if ((g.nslices == 6 || g.nslices == 7) && p->oz_pair_maps) {
+    } else if (oz_fixed_slices(g.nslices) && p->oz_pair_maps) {
       e = launch_oz_pair(g.nslices, a, p->oz_tmap, st);
       if (e != cudaSuccess) return fail(QS_ECUDA, std::string("CTA-pair GEMM launch: ") + cudaGetErrorString(e));
+    } else if (g.nslices == 4) {
+      oz_gemm_fixed_kernel<4, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices == 6) {
       oz_gemm_fixed_kernel<6, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
     } else if (g.nslices == 7) {

@@ -83,7 +83,7 @@ def test_slices_raised_until_accurate(qs, at, tmp_path):
 def test_float32_candidates_and_non_nest(qs, at, tmp_path):
     T32 = {("native", 1, False): 3.0, ("native", 2, False): 2.0, ("native", 3, False): 2.5,
            ("native", 4, False): 2.6,
-           ("bf16x3", 0, False): 2.2}
+           ("bf16x3", 0, False): 2.2, ("ozaki", 0, False): 2.4}
     t = at.Autotuner(qs, path=str(tmp_path / "f.json"), measure=fake(T32), device_name="B200")
     C, A, ia, B, ib, ic = views(qs, 300, 200, 20, dtype=torch.float32)
     assert t.options(C, A, ia, B, ib, ic) == {"method": "native", "native_tile": 2}
