@@ -76,7 +76,7 @@ enum { QS_ACC_NONE = 0, QS_ACC_F32 = 1, QS_ACC_F64 = 2 };
 enum {
   QS_METHOD_AUTO = 0,
   QS_METHOD_NATIVE = 1,   /* plain FP64 DMMA / FP32 FFMA gather kernel */
-  QS_METHOD_OZAKI_I8 = 2, /* FP64 as INT8 slices on tcgen05 kind::i8 */
+  QS_METHOD_OZAKI_I8 = 2, /* FP64 (6-7 digits) or FP32 (4 digits) as INT8 slices on tcgen05 kind::i8 */
   QS_METHOD_BF16X3 = 3    /* FP32 as split-BF16 x3 on tcgen05 kind::f16 */
 };
 
