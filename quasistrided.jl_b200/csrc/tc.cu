@@ -1429,6 +1429,8 @@ int tc_prepare(qs_plan *p) {
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_gemm_fixed_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1746,6 +1748,7 @@ __global__ void __launch_bounds__(256) oz_fixup_grouped(const FixupJob *jobs, in
 int tc_group_class(const qs_plan *p) {
   if (p->method == QS_METHOD_BF16X3) return TC_CLASS_BF16;
   if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) return TC_CLASS_I8;
+  if (p->tc.nslices == 4) return TC_CLASS_OZ4;
   if (p->tc.nslices == 6) return TC_CLASS_OZ6;
   if (p->tc.nslices == 7) return TC_CLASS_OZ7;
   return TC_CLASS_I8;
@@ -1858,7 +1861,9 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     oz_prep_grouped<<<pgrid, 256, 0, st>>>(zero, n);
     oz_rowmax_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
     oz_slice_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
-    if (g.cls == TC_CLASS_OZ6)
+    if (g.cls == TC_CLASS_OZ4)
+      oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
+    else if (g.cls == TC_CLASS_OZ6)
       oz_gemm_fixed_kernel<6, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
     else if (g.cls == TC_CLASS_OZ7)
       oz_gemm_fixed_kernel<7, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);

@@ -22,7 +22,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
                cudaStream_t st, cudaEvent_t *ev = nullptr);
 // Kernel class of a tensor-core plan in a grouped launch: plans of one class
 // share every launch of the class (pack, GEMM, fixup).
-enum { TC_CLASS_OZ6 = 0, TC_CLASS_OZ7 = 1, TC_CLASS_I8 = 2, TC_CLASS_BF16 = 3, TC_NCLASS = 4 };
+enum { TC_CLASS_OZ6 = 0, TC_CLASS_OZ7 = 1, TC_CLASS_I8 = 2, TC_CLASS_BF16 = 3, TC_CLASS_OZ4 = 4, TC_NCLASS = 5 };
 int tc_group_class(const qs_plan *p);
 
 // The device tables of one class of a grouped launch: a host image built by
