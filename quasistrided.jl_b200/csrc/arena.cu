@@ -44,7 +44,7 @@ struct qs_arena {
   // allocation below it reuses memory the device may still be using.
   size_t dirty = 0;
   int64_t waits = 0;
-  int device = 0;
+  int device = 0;  // -1: no CUDA device (bookkeeping only, nothing to order)
   bool owns = false;
   std::vector<Block> blocks;
   std::vector<cudaEvent_t> fences;  // recorded, not yet waited for
@@ -75,6 +75,7 @@ bool prune_fences(qs_arena *a) {
 
 // Records a fence on `stream` (caller holds the lock, current device set).
 int add_fence(qs_arena *a, void *stream) {
+  if (a->device < 0) return QS_OK;
   prune_fences(a);
   cudaEvent_t ev = nullptr;
   if (!a->spare.empty()) {
@@ -120,11 +121,14 @@ int wait_fences(qs_arena *a) {
 
 struct DeviceGuard {
   int prev = 0;
-  explicit DeviceGuard(int dev) {
+  bool on = false;
+  explicit DeviceGuard(int dev) : on(dev >= 0) {
+    if (!on) return;
     cudaGetDevice(&prev);
     if (prev != dev) cudaSetDevice(dev);
   }
   ~DeviceGuard() {
+    if (!on) return;
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != prev) cudaSetDevice(prev);
@@ -226,20 +230,37 @@ int qs_arena_create(qs_arena **out, void *base, size_t bytes) {
   qs_arena *a = new (std::nothrow) qs_arena();
   if (!a) return fail(QS_ENOMEM, "host allocation failed");
   cudaError_t e = cudaGetDevice(&a->device);
-  if (e == cudaSuccess && !base && bytes) {
+  if (e != cudaSuccess) {
+    // No device: only an arena over the caller's memory, as bookkeeping.
+    cudaGetLastError();
+    if (!base) {
+      delete a;
+      return fail(QS_ECUDA, std::string("device arena: ") + cudaGetErrorString(e));
+    }
+    a->device = -1;
+    a->base = static_cast<char *>(base);
+  } else if (base) {
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, base) != cudaSuccess ||
+        (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)) {
+      cudaGetLastError();
+      delete a;
+      return fail(QS_EINVAL, "ArgumentError: the arena's base is not device memory");
+    }
+    a->device = pa.device;
+    a->base = static_cast<char *>(base);
+  } else if (bytes) {
     void *p = nullptr;
     e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      delete a;
+      std::ostringstream m;
+      m << "device arena of " << bytes << " bytes: " << cudaGetErrorString(e);
+      return fail(QS_ENOMEM, m.str());
+    }
     a->base = static_cast<char *>(p);
     a->owns = true;
-  } else {
-    a->base = static_cast<char *>(base);
-  }
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    delete a;
-    std::ostringstream m;
-    m << "device arena of " << bytes << " bytes: " << cudaGetErrorString(e);
-    return fail(QS_ENOMEM, m.str());
   }
   a->cap = bytes;
   a->iface.ctx = a;
@@ -251,7 +272,7 @@ int qs_arena_create(qs_arena **out, void *base, size_t bytes) {
 
 int qs_arena_destroy(qs_arena *a) {
   if (!a) return QS_OK;
-  {
+  if (a->device >= 0) {
     std::lock_guard<std::mutex> lk(a->mu);
     DeviceGuard g(a->device);
     wait_fences(a);
