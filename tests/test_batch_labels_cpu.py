@@ -47,3 +47,22 @@ def test_batch_label_extent_and_bounds_errors(qs):
     p = qs.plan_contract(view(qs, (4, 6, 3), parent_len=4 * 6 * 3 - 1), view(qs, (4, 5, 3)), (1, 2, 9),
                          view(qs, (5, 6, 3)), (2, 3, 9), (1, 3, 9), host_only=True, batch_labels=True)
     assert not p.bounds_ok
+
+
+def test_batch_bounds_with_negative_stride_and_swap(qs):
+    # C's batch axis runs backwards from an offset: in bounds only when the
+    # offset covers the negative span.
+    par = torch.zeros(4 * 6 * 3, dtype=torch.float64)
+    A, B = view(qs, (4, 5, 3)), view(qs, (5, 6, 3))
+    ok = qs.StridedView(par, (4, 6, 3), (1, 4, -24), 48)
+    p = qs.plan_contract(ok, A, (1, 2, 9), B, (2, 3, 9), (1, 3, 9), host_only=True, batch_labels=True)
+    assert p.bounds_ok and p.batch_length == 3
+    bad = qs.StridedView(par, (4, 6, 3), (1, 4, -24), 24)
+    p = qs.plan_contract(bad, A, (1, 2, 9), B, (2, 3, 9), (1, 3, 9), host_only=True, batch_labels=True)
+    assert not p.bounds_ok
+    # C row-major in (i, j): the N side has C's unit stride, so A and B swap roles;
+    # the batch label stays a batch label.
+    Ct = qs.StridedView(torch.zeros(4 * 64 * 3, dtype=torch.float64), (4, 64, 3), (64, 1, 256))
+    Bw = view(qs, (5, 64, 3))
+    p = qs.plan_contract(Ct, A, (1, 2, 9), Bw, (2, 3, 9), (1, 3, 9), host_only=True, batch_labels=True)
+    assert p.swapped and p.batch_labels == (9,) and p.bounds_ok
