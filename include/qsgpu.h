@@ -6,13 +6,13 @@
  * the semantics of QuasiStrided.jl's engine:
  *
  *   plan_contract  src/planning/plan.jl:115-133   -> qs_plan_contract
- *   execute!       src/execution/execute.jl:191   -> qs_execute
- *   contract!      src/execution/execute.jl:264   -> qs_contract
+ *   execute!       src/execution/execute.jl:11   -> qs_execute
+ *   contract!      src/execution/execute.jl:84   -> qs_contract
  *   release!       src/execution/workspace.jl:118 -> qs_plan_destroy
  *   QuasiStridedBackend(; accumulator)            -> qs_plan_options.accumulator
- *     src/integrations/tensoroperations.jl:299-307
+ *     src/integrations/tensoroperations.jl:24-32
  *   TO.tensorcontract! label mapping              -> qs_contraction_labels
- *     src/integrations/tensoroperations.jl:315-322
+ *     src/integrations/tensoroperations.jl:40-47
  *   TO.tensoradd! / TO.tensortrace! (forwarded to StridedNative there)
  *     src/integrations/tensoroperations.jl:91-107  -> qs_tensoradd_trace
  *   TensorOperations allocators for the workspace -> qs_plan_options.allocator,
@@ -31,8 +31,9 @@
  *    `convert(T, alpha)` throws InexactError).
  *  - Every validation happens before anything is written: plan-time errors
  *    come from qs_plan_contract, out-of-bounds operands from qs_execute before
- *    any launch (src/execution/execute.jl:182-189,
- *    test/execution/test_execute.jl:334-347).
+ *    any launch (the reference checks spans with checked_span_bounds,
+ *    src/layout/tiles.jl:123-140, before a block is written;
+ *    test/execution/test_execute.jl:57-70).
  *  - No C++ exception crosses this boundary.  The message of the last error
  *    on the calling thread is available from qs_last_error.
  *  - A plan borrows the operands' device memory and owns its device
@@ -196,13 +197,13 @@ int qs_plan_contract(qs_plan **plan, const qs_view *C, const qs_view *A,
                      const int64_t *indB, const int64_t *indC,
                      const qs_plan_options *opts);
 
-/* execute! (src/execution/execute.jl:191-200): alpha/beta are {re, im}.
+/* execute! (src/execution/execute.jl:11-20): alpha/beta are {re, im}.
  * stream is a cudaStream_t (NULL = legacy default stream).  Asynchronous:
  * returns once the work is enqueued. */
 int qs_execute(qs_plan *plan, const double *alpha, const double *beta,
                void *stream);
 
-/* contract! (src/execution/execute.jl:264-275): plan, execute, release in one
+/* contract! (src/execution/execute.jl:84-95): plan, execute, release in one
  * call.  The plan's workspace is freed stream-ordered after the work: with
  * the library's pool the call waits for `stream`; with opts->allocator it
  * returns once the work is enqueued and hands the workspace back with
@@ -223,7 +224,7 @@ int qs_plan_get_info(const qs_plan *plan, qs_plan_info *info);
  * storages the same way.  Used by the serving loop to reuse plans. */
 int qs_plan_rebind(qs_plan *plan, void *A_data, void *B_data, void *C_data);
 
-/* TO.tensorcontract! label mapping (src/integrations/tensoroperations.jl:315-322):
+/* TO.tensorcontract! label mapping (src/integrations/tensoroperations.jl:40-47):
  * pA = (pA_out[NoA], pA_in[Nk]), pB = (pB_in[Nk], pB_out[NoB]),
  * pAB = (pAB_1 ++ pAB_2)[NoA+NoB], all 1-based as in Julia.  Writes
  * indA[NoA+Nk], indB[Nk+NoB], indC[NoA+NoB]. */
@@ -235,7 +236,7 @@ int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB,
 /* Grouped execution of many independent plans: the block-sparse
  * contraction step of a symmetric tensor network, where each charge sector
  * is one plan.  No counterpart in the reference, whose engine runs one plan
- * per contract! call (src/execution/execute.jl:191-210); each plan's result
+ * per contract! call (src/execution/execute.jl:84-95); each plan's result
  * is that of qs_execute on it.
  *
  * Modes:

@@ -7,14 +7,14 @@ this module           QuasiStrided.jl
 ====================  ==========================================================
 ``StridedView``       ``StridedViews.StridedView`` (parent, size, strides, offset, op)
 ``plan_contract``     ``plan_contract`` (src/planning/plan.jl:115-133)
-``execute``           ``execute!`` (src/execution/execute.jl:191-200)
-``contract``          ``contract!`` (src/execution/execute.jl:264-275)
+``execute``           ``execute!`` (src/execution/execute.jl:11-20)
+``contract``          ``contract!`` (src/execution/execute.jl:84-95)
 ``ContractPlan``      ``ContractPlan`` (src/planning/plan.jl:16-45)
 ``release``           ``release!`` (src/execution/workspace.jl:118-123)
 ``PathModes``         ``PathModes`` (src/planning/plan.jl:60-64)
-``QuasiStridedBackend``  ``QuasiStridedBackend`` (src/integrations/tensoroperations.jl:299-307)
-``tensorcontract``    ``TO.tensorcontract!`` method (tensoroperations.jl:350-363)
-``contraction_labels``  ``contraction_labels`` (tensoroperations.jl:315-322)
+``QuasiStridedBackend``  ``QuasiStridedBackend`` (src/integrations/tensoroperations.jl:24-32)
+``tensorcontract``    ``TO.tensorcontract!`` method (tensoroperations.jl:75-88)
+``contraction_labels``  ``contraction_labels`` (tensoroperations.jl:40-47)
 ====================  ==========================================================
 
 Operands are ``StridedView`` s over torch tensors in device memory.  All

@@ -1,8 +1,8 @@
 // The C ABI (include/qsgpu.h): plan creation, execution and destruction.
 //
 //   qs_plan_contract <- plan_contract / planned (src/planning/plan.jl:115-262)
-//   qs_execute       <- execute! (src/execution/execute.jl:191-210)
-//   qs_contract      <- contract! (src/execution/execute.jl:264-275)
+//   qs_execute       <- execute! (src/execution/execute.jl:11-20)
+//   qs_contract      <- contract! (src/execution/execute.jl:84-95)
 //   qs_plan_destroy  <- release! (src/execution/workspace.jl:118-123)
 //
 // All validation happens on the host before anything is written; kernels
@@ -682,7 +682,7 @@ int qs_plan_rebind(qs_plan *p, void *A_data, void *B_data, void *C_data) {
 int qs_contraction_labels(int32_t NoA, int32_t Nk, int32_t NoB, const int64_t *pA_lin,
                           const int64_t *pB_lin, const int64_t *pAB_lin, int64_t *indA,
                           int64_t *indB, int64_t *indC) {
-  // TO's pA/pB/pAB -> one label per axis (src/integrations/tensoroperations.jl:315-322):
+  // TO's pA/pB/pAB -> one label per axis (src/integrations/tensoroperations.jl:40-47):
   // 1:NoA for A's open axes (pA[1] order), NoA+1:NoA+NoB for B's open axes,
   // -1:-1:-Nk for the contracted pairs; indC = linearize(pAB).
   if (NoA < 0 || Nk < 0 || NoB < 0) return fail(QS_EINVAL, "ArgumentError: negative counts");

@@ -6,7 +6,7 @@
 //                    src/microkernels/steps.jl:27-36): acc = muladd(a, b, acc)
 //                    ascending in the plan's K order; complex in the planar
 //                    kernel's fused order (steps.jl:121-167)
-//   scale         <- scale_all_of_C! (src/execution/execute.jl:214-245)
+//   scale         <- scale_all_of_C! (src/execution/execute.jl:34-57)
 //   dot           <- execute_path!(DotPath) (src/execution/dot.jl:13-76)
 //   outer         <- execute_path!(OuterPath) (src/execution/outer.jl:10-69)
 #include <cuda_runtime.h>

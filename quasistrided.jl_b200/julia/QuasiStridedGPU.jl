@@ -178,7 +178,7 @@ end
 """
     execute!(plan, alpha, beta) -> parent(C)
 
-QuasiStrided.execute! (src/execution/execute.jl:191): enqueued on CUDA.jl's
+QuasiStrided.execute! (src/execution/execute.jl:11): enqueued on CUDA.jl's
 current stream.
 """
 function execute!(p::ContractPlan, alpha::Number, beta::Number)
@@ -197,7 +197,7 @@ function contract!(C::DeviceStridedView, alpha::Number, A::DeviceStridedView, in
         indB, beta::Number, indC; accumulator = nothing)
     p = plan_contract(C, A, indA, B, indB, indC; accumulator)
     execute!(p, alpha, beta)
-    CUDA.synchronize()
+    CUDA.synchronize()  # the plan's workspace goes back to the pool below
     release!(p)
     return C
 end
@@ -206,7 +206,7 @@ end
     QuasiStridedGPUBackend(; accumulator = nothing)
 
 The device counterpart of QuasiStridedBackend
-(src/integrations/tensoroperations.jl:299-307).
+(src/integrations/tensoroperations.jl:24-32).
 """
 struct QuasiStridedGPUBackend{A} <: TO.AbstractBackend
     function QuasiStridedGPUBackend{A}() where {A}
@@ -220,6 +220,9 @@ QuasiStridedGPUBackend(; accumulator = nothing) = QuasiStridedGPUBackend{accumul
 function TO.tensorcontract!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::Bool,
         B::CuArray, pB::TO.Index2Tuple, conjB::Bool, pAB::TO.Index2Tuple,
         α::Number, β::Number, ::QuasiStridedGPUBackend{AC}, allocator = TO.DefaultAllocator()) where {AC}
+    # prepare_contraction's checks (src/integrations/tensoroperations.jl:61-70)
+    TO.argcheck_tensorcontract(C, A, pA, B, pB, pAB)
+    TO.dimcheck_tensorcontract(C, A, pA, B, pB, pAB)
     NoA, Nk, NoB = length(pA[1]), length(pA[2]), length(pB[2])
     lin(p) = Int64[p[1]..., p[2]...]
     indA = Vector{Int64}(undef, NoA + Nk)
@@ -270,8 +273,7 @@ function TO.tensoradd!(C::CuArray, A::CuArray, pA::TO.Index2Tuple, conjA::Bool, 
         indA[ax] = i
     end
     add_trace!(DeviceStridedView(C), α, DeviceStridedView(A), indA, β, 1:ndims(C); conjA)
-    CUDA.synchronize()
-    return C
+    return C  # stream-ordered: later work on CUDA.jl's stream sees C
 end
 
 # TO.tensortrace!: C = β C + α (trace of op(A) over the pairs (q[1][j], q[2][j]),
@@ -286,8 +288,7 @@ function TO.tensortrace!(C::CuArray, A::CuArray, p::TO.Index2Tuple, q::TO.Index2
         indA[x] = indA[y] = -j
     end
     add_trace!(DeviceStridedView(C), α, DeviceStridedView(A), indA, β, 1:ndims(C); conjA)
-    CUDA.synchronize()
-    return C
+    return C  # stream-ordered: later work on CUDA.jl's stream sees C
 end
 
 end # module

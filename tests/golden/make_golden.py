@@ -12,7 +12,7 @@ by this engine or by the oracle:
   order_free_labels.json  test/planning/test_labels.jl:26-50
   leading_unit_run.json   test/planning/test_labels.jl:52-75
   axis_group.json         test/layout/test_axis_group.jl:14-26
-  contraction_labels.json src/integrations/tensoroperations.jl:309-313 (worked example)
+  contraction_labels.json src/integrations/tensoroperations.jl:34-38 (worked example)
   label_errors.json       test/planning/test_plan.jl:3-35, test/planning/test_labels.jl:19-23
 
 Julia is not available where this runs, so the reference's tests cannot be
