@@ -188,16 +188,15 @@ int arena_free(qs_arena *a, void *ptr, size_t bytes, void *stream) {
   auto it = std::find_if(a->blocks.begin(), a->blocks.end(), [&](const Block &b) { return b.off == off; });
   if (it == a->blocks.end()) return QS_OK;  // already reclaimed by a reset
   it->freed = true;
-  const size_t before = a->top;
   while (!a->blocks.empty() && a->blocks.back().freed) {
     a->top = a->blocks.back().off;
     a->blocks.pop_back();
   }
-  if (a->top < before) {
-    DeviceGuard g(a->device);
-    return add_fence(a, stream);
-  }
-  return QS_OK;
+  // The fence goes on this free's stream whether the block popped now or
+  // only got marked: a marked block is popped later by a free on another
+  // stream, whose fence says nothing about the work on this one.
+  DeviceGuard g(a->device);
+  return add_fence(a, stream);
 }
 
 void *iface_alloc(void *ctx, size_t bytes) {

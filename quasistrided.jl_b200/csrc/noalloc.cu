@@ -96,17 +96,6 @@ __global__ void noalloc_fill_offsets(const __grid_constant__ FillArgs a) {
   }
 }
 
-int case_of(int T, const double *v) {
-  double re = v[0], im = is_complex(T) ? v[1] : 0.0;
-  if (!is_double(T)) {
-    re = (double)(float)re;
-    im = (double)(float)im;
-  }
-  if (re == 0.0 && im == 0.0) return 0;
-  if (re == 1.0 && im == 0.0) return 1;
-  return 2;
-}
-
 }  // namespace
 }  // namespace qs
 
@@ -134,9 +123,12 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
       << "static scratch holds at most " << kNoAllocEntries << " — use qs_plan_contract/qs_execute";
     return fail(QS_EINVAL, s.str());
   }
-  const int acase = case_of(p.T, alpha), bcase = case_of(p.T, beta);
+  const int nt = o.native_tile;
+  if (nt < 0 || nt > 4) return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..4");
+  const int acase = scalar_case(p.T, alpha), bcase = scalar_case(p.T, beta);
   const bool scale_only = acase == 0 || p.path == QS_PATH_SCALE;
   if ((rc = check_bounds(&p, !scale_only))) return rc;
+  if (scale_only && bcase == 1) return QS_OK;  // C *= 1: nothing to launch, as qs_execute
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(QS_ECUDA, "cudaGetDevice failed");
@@ -179,13 +171,15 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
   op.N = p.N;
   op.K = p.K;
   if (scale_only) {
-    if (bcase != 1) e = launch_scale(p.T, op, beta, bcase, p.c_mfast, st);
+    e = launch_scale(p.T, op, beta, bcase, p.c_mfast, st);
   } else if (p.path == QS_PATH_DOT) {
     e = launch_dot(p.T, op, alpha, beta, bcase, st);
   } else if (p.path == QS_PATH_OUTER) {
     e = launch_outer(p.T, op, alpha, beta, bcase, p.c_mfast, st);
   } else {
-    e = launch_direct(p.T, op, alpha, beta, bcase, p.a_mfast, p.b_nfast, direct_shape(p.T, p.N), st);
+    // The tile shape qs_plan_contract would give the same problem.
+    const int shape = (nt > 0 && !is_complex(p.T)) ? nt - 1 : direct_shape_mn(p.T, p.M, p.N);
+    e = launch_direct(p.T, op, alpha, beta, bcase, p.a_mfast, p.b_nfast, shape, st);
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -193,6 +187,6 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
     s << "CUDA error in qs_contract_noalloc: " << cudaGetErrorString(e);
     return fail(QS_ECUDA, s.str());
   }
-  count_launches(2);
+  count_launches(2);  // the offset fill and one kernel
   return QS_OK;
 }

@@ -142,3 +142,28 @@ def test_grouped_plans_from_an_arena(qs):
     for A, B, C in outs:
         assert torch.allclose(C, A @ B, rtol=1e-12, atol=1e-10)
     assert arena.info()["used"] == 0
+
+
+def test_marked_free_keeps_its_stream_fence(qs):
+    # A lower block freed on stream S1 is only marked; the top block freed on
+    # an idle stream S2 then pops both.  The memory must not come back before
+    # S1's work is done: qs_arena_alloc (a host-side tensoralloc) waits for it.
+    arena = qs.DeviceArena(1 << 20)
+    low = arena.alloc(4096)
+    top = arena.alloc(4096)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    with torch.cuda.stream(s1):
+        torch.cuda._sleep(200_000_000)   # ~0.1 s of device time that "uses" `low`
+        done = torch.cuda.Event()
+        done.record(s1)
+    arena.free(low, 4096, s1)
+    assert arena.info()["used"] > 0      # marked, not popped
+    arena.free(top, 4096, s2)
+    assert arena.info()["used"] == 0     # popped together
+    again = arena.alloc(4096)
+    assert again == low
+    assert done.query(), "arena handed back memory while S1's work was still running"
+    assert arena.info()["waits"] >= 1
+    arena.free(again, 4096)
+    torch.cuda.synchronize()
+    arena.close()

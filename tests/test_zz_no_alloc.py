@@ -72,3 +72,24 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     C = qs.StridedView(torch.zeros(1, dtype=torch.float64, device="cuda"), (), (), 0)
     with pytest.raises(qs.ArgumentError, match="static scratch"):
         _noalloc(qs, C, 1.0, big, (1,), v, (1,), 0.0, ())
+
+
+def test_noalloc_scale_dot_outer_paths():
+    # The other paths the entry point serves, each against plan_contract +
+    # execute on the same problem: alpha == 0 (C *= beta, A and B unread),
+    # beta == 1 with alpha == 0 (nothing launched), an empty K (C *= beta),
+    # a dot shape (M == 1) and an outer product (no K).
+    from conftest import load_engine
+    qs = load_engine()
+    rng = np.random.default_rng(77)
+    eps64 = float(np.finfo(np.float64).eps)
+    mm = ((40, 30), (30, 20), (40, 20))
+    for alpha, beta in ((0.0, 0.5), (0.0, 1.0), (0.0, 0.0)):
+        ref, got, _ = _case(qs, rng, mm, ((1, 2), (2, 3), (1, 3)), "Float64", alpha, beta)
+        assert np.array_equal(got, ref)
+    ref, got, _ = _case(qs, rng, ((40, 0), (0, 20), (40, 20)), ((1, 2), (2, 3), (1, 3)), "Float64", 1.5, 0.5)
+    assert np.array_equal(got, ref)
+    ref, got, K = _case(qs, rng, ((1, 700), (700, 29), (1, 29)), ((1, 2), (2, 3), (1, 3)), "Float64", 1.5, 0.5)
+    assert rel_fro(got, ref) <= 10 * np.sqrt(K) * eps64
+    ref, got, _ = _case(qs, rng, ((37,), (21,), (37, 21)), ((1,), (2,), (1, 2)), "ComplexF64", 1.5, 0.5)
+    assert rel_fro(got, ref) <= 4 * eps64
