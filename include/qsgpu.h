@@ -76,7 +76,9 @@ enum { QS_ACC_NONE = 0, QS_ACC_F32 = 1, QS_ACC_F64 = 2 };
 /* GEMM method for the nest path.  AUTO follows the autotuner's choice. */
 enum {
   QS_METHOD_AUTO = 0,
-  QS_METHOD_NATIVE = 1,   /* plain FP64 DMMA / FP32 FFMA gather kernel */
+  QS_METHOD_NATIVE = 1,   /* gather GEMM without tensor-core splitting: real Float64
+                             operands on the FP64 tensor cores (DMMA, mma.sync f64),
+                             other types as a SIMT FMA kernel */
   QS_METHOD_OZAKI_I8 = 2, /* FP64 (6-7 digits) or FP32 (4 digits) as INT8 slices on tcgen05 kind::i8 */
   QS_METHOD_BF16X3 = 3    /* FP32 as split-BF16 x3 on tcgen05 kind::f16 */
 };
@@ -159,9 +161,11 @@ typedef struct qs_plan_options {
   int32_t ozaki_slices;    /* 0 = chosen from K for 1e-13; else 2..10 */
   int32_t complex_mode;    /* QS_CPLX_*; 0 = default for the method */
   int32_t flags;           /* QS_PLAN_* */
-  int32_t native_tile;     /* gather-GEMM tile: 0 = by M and N; 1 = 64x64, 2 = 128x32,
-                              3 = 256x16, 4 = 32x32 (real compute types; the
-                              autotuner's knob) */
+  int32_t native_tile;     /* native-method tile: 0 = by M and N; SIMT gather kernel
+                              1 = 64x64, 2 = 128x32, 3 = 256x16, 4 = 32x32 (real
+                              compute types); DMMA kernel (real Float64 A and B)
+                              5 = 128x128, 6 = 128x64, 7 = 64x64, 8 = 128x32,
+                              9 = 256x16 (the autotuner's knob) */
   const qs_allocator *allocator; /* plan workspace from here; NULL = the library's
                                     stream-ordered pool (DefaultAllocator) */
 } qs_plan_options;
@@ -182,7 +186,7 @@ typedef struct qs_plan_info {
   int64_t workspace_bytes;
   int32_t stride_class;  /* bit 0: A's M map unit-stride, bit 1: B's N map,
                             bit 2: C's M map (the autotuner's stride class) */
-  int32_t native_tile;   /* gather-GEMM tile in use (1..4 as in the options) */
+  int32_t native_tile;   /* native-method tile in use (1..9 as in the options) */
   int32_t batch_rank;    /* batch labels (QS_PLAN_BATCH_LABELS), 0 without */
   int64_t batch_length;  /* product of their extents (1 without) */
   int64_t batch_labels[16];

@@ -93,12 +93,16 @@ class Autotuner:
 
     # ------------------------------------------------------ candidates ---
     @staticmethod
-    def candidates(hp) -> list:
+    def candidates(hp, dmma: bool = False) -> list:
+        """Options to time for a problem class; `dmma`: A and B are real
+        Float64 in a Float64 computation, so the DMMA kernel's tiles
+        (native_tile 5..9) are candidates beside the SIMT tiles (1..4)."""
         real = not hp.compute_type.startswith("Complex")
         dbl = hp.compute_type in ("Float64", "ComplexF64")
         out = []
         if real:
-            out += [{"method": "native", "native_tile": t} for t in (1, 2, 3, 4)]
+            tiles = (1, 2, 3, 4, 5, 6, 7, 8, 9) if dmma else (1, 2, 3, 4)
+            out += [{"method": "native", "native_tile": t} for t in tiles]
         else:
             out.append({"method": "native"})
         out.append({"method": "ozaki"})
@@ -171,7 +175,10 @@ class Autotuner:
         target = 1e-13 if hp.compute_type in ("Float64", "ComplexF64") else 1e-5
         ref_store = {}
         results = []
-        for cand in self.candidates(hp):
+        import torch
+        dmma = (hp.compute_type == "Float64" and A.parent.dtype == torch.float64
+                and B.parent.dtype == torch.float64)
+        for cand in self.candidates(hp, dmma):
             opts = dict(cand)
             while True:
                 if self._measure is not None:

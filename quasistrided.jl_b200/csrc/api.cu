@@ -426,11 +426,11 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
     p->method = QS_METHOD_NATIVE;
   }
   const int nt = p->opts.native_tile;
-  if (nt < 0 || nt > 4) {
+  if (nt < 0 || nt > kNativeShapes) {
     delete p;
-    return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..4");
+    return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..9");
   }
-  p->native_shape = (nt > 0 && !is_complex(p->T)) ? nt - 1 : direct_shape_mn(p->T, p->M, p->N);
+  p->native_shape = native_shape_for(p->T, p->TA, p->TB, p->M, p->N, p->K, nt, false);
   if (!p->host_only) {
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) {

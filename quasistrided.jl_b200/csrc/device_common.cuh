@@ -188,4 +188,33 @@ __device__ __forceinline__ T axpby(const Scalars<T> &s, T r, T old) {
   return cfma(s.alpha, r, cmul(s.beta, old));
 }
 
+// Host: alpha/beta ({re, im} doubles) in compute type T.
+template <class T>
+inline Scalars<T> make_scalars(const double *alpha, const double *beta, int beta_case) {
+  Scalars<T> s;
+  if constexpr (is_cplx<T>::value) {
+    using R = typename real_of<T>::type;
+    s.alpha.re = (R)alpha[0];
+    s.alpha.im = (R)alpha[1];
+    s.beta.re = (R)beta[0];
+    s.beta.im = (R)beta[1];
+  } else {
+    s.alpha = (T)alpha[0];
+    s.beta = (T)beta[0];
+  }
+  s.beta_case = beta_case;
+  return s;
+}
+
+// One problem of a grouped gather-GEMM launch: a CTA finds the job whose
+// block range holds its index and runs tile (lb % gx, lb / gx) of it.
+template <class T>
+struct NativeJob {
+  Operands op;
+  Scalars<T> s;
+  int a_mfast, b_nfast;
+  int gx;  // tiles along M
+  int block_start;
+};
+
 }  // namespace qs

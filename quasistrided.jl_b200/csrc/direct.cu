@@ -213,17 +213,8 @@ int direct_shape(int T, int64_t N) {
 }
 
 // Grouped: CTA b runs tile b - block_start of the problem whose block range
-// holds b (binary search over the table); problems sorted by K descending
-// so that the longest tiles start first.
-template <class T>
-struct NativeJob {
-  Operands op;
-  Scalars<T> s;
-  int a_mfast, b_nfast;
-  int gx;  // tiles along M
-  int block_start;
-};
-
+// holds b (binary search over the NativeJob table); problems sorted by K
+// descending so that the longest tiles start first.
 template <class T, class Cfg>
 __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJob<T> *jobs, int njobs) {
   int lo = 0, hi = njobs - 1;
@@ -247,6 +238,16 @@ __global__ void __launch_bounds__(256) direct_gemm_grouped_kernel(const NativeJo
 // the tiled kernel).  Bandwidth-bound: A is read once and C written once,
 // with no tile padding along N.
 constexpr int kSkinnyN = 16, kSkinnyK = 64;
+
+int native_shape_for(int T, int TA, int TB, int64_t M, int64_t N, int64_t K, int native_tile, bool grouped) {
+  // Problems the skinny kernel takes alone stay on the SIMT tiles in a
+  // group too, so that a group's result equals its plans' own results.
+  const bool dmma = dmma_eligible(T, TA, TB) && !(N <= kSkinnyN && K <= kSkinnyK);
+  if (native_tile >= 1 && native_tile <= kSimtShapes) return is_complex(T) ? 0 : native_tile - 1;
+  if (native_tile > kSimtShapes && native_tile <= kNativeShapes && dmma) return native_tile - 1;
+  if (dmma) return kSimtShapes + (grouped ? dmma_shape_n(N) : dmma_shape_mn(M, N));
+  return grouped ? direct_shape(T, N) : direct_shape_mn(T, M, N);
+}
 
 template <class T>
 __device__ __forceinline__ void skinny_entry(const Operands &op, const Scalars<T> &s, T *Bs, int64_t *sKA,
@@ -413,23 +414,6 @@ static int grid_for(int64_t work, int threads) {
 }
 
 template <class T>
-static Scalars<T> make_scalars(const double *alpha, const double *beta, int beta_case) {
-  Scalars<T> s;
-  if constexpr (is_cplx<T>::value) {
-    using R = typename real_of<T>::type;
-    s.alpha.re = (R)alpha[0];
-    s.alpha.im = (R)alpha[1];
-    s.beta.re = (R)beta[0];
-    s.beta.im = (R)beta[1];
-  } else {
-    s.alpha = (T)alpha[0];
-    s.beta = (T)beta[0];
-  }
-  s.beta_case = beta_case;
-  return s;
-}
-
-template <class T>
 static cudaError_t launch_scale_t(const Operands &op, const double *alpha, const double *beta,
                                   int beta_case, int mfast, cudaStream_t st) {
   auto s = make_scalars<T>(alpha, beta, beta_case);
@@ -482,6 +466,9 @@ static cudaError_t launch_direct_t(int shape, const Operands &op, const double *
 
 cudaError_t launch_direct(int T, const Operands &op, const double *alpha, const double *beta,
                           int beta_case, int a_mfast, int b_nfast, int shape, cudaStream_t st) {
+  if (shape >= kSimtShapes && dmma_eligible(T, op.TA, op.TB) && !(op.N <= kSkinnyN && op.K <= kSkinnyK))
+    return launch_dmma(op, alpha, beta, beta_case, a_mfast, b_nfast, shape - kSimtShapes, st);
+  if (shape >= kSimtShapes) shape = 0;
   switch (T) {
     case QS_F32: return launch_direct_t<float>(shape, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
     case QS_F64: return launch_direct_t<double>(shape, op, alpha, beta, beta_case, a_mfast, b_nfast, st);
@@ -560,7 +547,8 @@ static int native_group_build_t(NativeGroup &g, const Operands *ops, const doubl
     j.a_mfast = g.plans[i]->a_mfast;
     j.b_nfast = g.plans[i]->b_nfast;
     int bm = 64, bn = 64;
-    if (is_complex(g.T)) bm = bn = 32;
+    if (g.shape >= kSimtShapes) dmma_tile_dims(g.shape - kSimtShapes, &bm, &bn);
+    else if (is_complex(g.T)) bm = bn = 32;
     else if (g.shape == 1) bm = 128, bn = 32;
     else if (g.shape == 2) bm = 256, bn = 16;
     else if (g.shape == 3) bm = 32, bn = 32;
@@ -605,6 +593,8 @@ static cudaError_t native_group_launch_t(const NativeGroup &g, cudaStream_t st) 
 
 cudaError_t native_group_launch(const NativeGroup &g, cudaStream_t st) {
   if (g.plans.empty()) return cudaSuccess;
+  if (g.shape >= kSimtShapes)
+    return dmma_group_launch(g.shape - kSimtShapes, g.dev, (int)g.plans.size(), g.blocks, st);
   switch (g.T) {
     case QS_F32: return native_group_launch_t<float>(g, st);
     case QS_F64: return native_group_launch_t<double>(g, st);

@@ -25,7 +25,7 @@ struct qs_group {
   int mode = QS_GROUP_PERSISTENT;
   std::vector<qs_plan *> plans;
   // Persistent mode: the classes and the plans that run on their own.
-  NativeGroup native[16];  // by compute type QS_F32..QS_C64 x tile shape
+  NativeGroup native[4 * kNativeShapes];  // by compute type QS_F32..QS_C64 x native shape
   TcGroup tc[TC_NCLASS];
   std::vector<int> single;
   bool built = false;
@@ -106,7 +106,7 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
   release_tables(g);
   const int n = (int)g->plans.size();
   std::vector<int> bcase(n);
-  std::vector<std::vector<int>> nat(16), tcm(TC_NCLASS);
+  std::vector<std::vector<int>> nat(4 * kNativeShapes), tcm(TC_NCLASS);
   for (int i = 0; i < n; ++i) {
     qs_plan *p = g->plans[i];
     const int acase = scalar_case(p->T, alpha + 2 * i);
@@ -118,9 +118,10 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
       // The 32x32 tile exists to fill the GPU with one small problem; in a
       // group the other problems fill it, so the N-based shape is used unless
       // the plan asked for 32x32 itself.
-      const int sh = (p->native_shape == 3 && p->opts.native_tile == 0) ? direct_shape(p->T, p->N)
-                                                                         : p->native_shape;
-      nat[4 * (p->T - QS_F32) + sh].push_back(i);
+      const int sh = p->opts.native_tile == 0
+                         ? native_shape_for(p->T, p->TA, p->TB, p->M, p->N, p->K, 0, true)
+                         : p->native_shape;
+      nat[kNativeShapes * (p->T - QS_F32) + sh].push_back(i);
     } else {
       tcm[tc_group_class(p)].push_back(i);
     }
@@ -131,12 +132,12 @@ int build_tables(qs_group *g, const double *alpha, const double *beta, cudaStrea
     });
   };
   int rc;
-  for (int t = 0; t < 16; ++t) {
+  for (int t = 0; t < 4 * kNativeShapes; ++t) {
     if (nat[t].empty()) continue;
     by_cost(nat[t]);
     NativeGroup &c = g->native[t];
-    c.T = QS_F32 + t / 4;
-    c.shape = t % 4;
+    c.T = QS_F32 + t / kNativeShapes;
+    c.shape = t % kNativeShapes;
     std::vector<Operands> ops;
     for (int i : nat[t]) {
       c.plans.push_back(g->plans[i]);

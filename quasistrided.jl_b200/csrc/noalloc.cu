@@ -124,7 +124,7 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
     return fail(QS_EINVAL, s.str());
   }
   const int nt = o.native_tile;
-  if (nt < 0 || nt > 4) return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..4");
+  if (nt < 0 || nt > kNativeShapes) return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..9");
   const int acase = scalar_case(p.T, alpha), bcase = scalar_case(p.T, beta);
   const bool scale_only = acase == 0 || p.path == QS_PATH_SCALE;
   if ((rc = check_bounds(&p, !scale_only))) return rc;
@@ -177,8 +177,8 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
   } else if (p.path == QS_PATH_OUTER) {
     e = launch_outer(p.T, op, alpha, beta, bcase, p.c_mfast, st);
   } else {
-    // The tile shape qs_plan_contract would give the same problem.
-    const int shape = (nt > 0 && !is_complex(p.T)) ? nt - 1 : direct_shape_mn(p.T, p.M, p.N);
+    // The kernel and tile shape qs_plan_contract would give the same problem.
+    const int shape = native_shape_for(p.T, p.TA, p.TB, p.M, p.N, p.K, nt, false);
     e = launch_direct(p.T, op, alpha, beta, bcase, p.a_mfast, p.b_nfast, shape, st);
   }
   if (e == cudaSuccess) e = cudaGetLastError();

@@ -1,7 +1,8 @@
 """GPU tests of the autotuner: it measures every candidate on scratch data
 of the problem's layout, picks one that meets the accuracy target, caches it
-on disk, and the tuned plan matches the oracle; every gather-GEMM tile
-shape it can pick is bitwise equal to the oracle."""
+on disk, and the tuned plan matches the oracle; every SIMT gather-GEMM
+tile shape it can pick is bitwise equal to the oracle, every DMMA tile
+within the reference's 50*K*eps."""
 import importlib
 import json
 
@@ -48,3 +49,17 @@ def test_native_tile_override_bitwise(qs, orc, tile):
                               native_tile=tile)
     assert plan.native_tile == tile
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("tile", [5, 6, 7, 8, 9])
+def test_native_tile_override_dmma(qs, orc, tile):
+    # The DMMA kernel's tiles (native_tile 5..9), the autotuner's other knob.
+    rng = np.random.default_rng(tile)
+    M, K, N = 333, 97, 45
+    A = colmajor_pair(qs, rng, (M, K), "Float64")
+    B = colmajor_pair(qs, rng, (K, N), "Float64")
+    C = colmajor_pair(qs, rng, (M, N), "Float64")
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native",
+                              native_tile=tile)
+    assert plan.native_tile == tile
+    assert rel_fro(got, ref) <= 50 * K * np.finfo(np.float64).eps

@@ -56,13 +56,19 @@ def test_batched_matmul_bitwise(qs, orc, et, ab):
     A = colmajor_pair(qs, rng, (M, K, P), et)
     B = colmajor_pair(qs, rng, (K, N, P), et)
     C = colmajor_pair(qs, rng, (M, N, P), et, fill=np.nan if ab[1] == 0 else None)
+    C0 = C.host.parent.copy()
     got, want, plan = run(qs, orc, C, ab[0], A, (1, 2, 9), B, (2, 3, 9), ab[1], (1, 3, 9), [9], [P],
                           method="native")
     assert plan.batch_length == P and plan.method == "native"
+    eps = np.finfo(np.float64 if et == "Float64" else np.float32).eps
+    assert rel_fro(got, want) <= 50 * K * eps   # Float64: the DMMA kernel over grid z
     if et == "Float64":
-        assert np.array_equal(got, want)      # the ScalarKernel FMA order, per entry
-    else:
-        assert rel_fro(got, want) <= 50 * K * np.finfo(np.float32).eps
+        # the SIMT tile keeps the ScalarKernel FMA order, per entry
+        C.host.parent[:] = C0
+        C.dev.parent.copy_(torch.from_numpy(C0))
+        got, want, plan = run(qs, orc, C, ab[0], A, (1, 2, 9), B, (2, 3, 9), ab[1], (1, 3, 9), [9], [P],
+                              method="native", native_tile=1)
+        assert np.array_equal(got, want)
 
 
 def test_two_batch_labels_strided_conj_complex(qs, orc):

@@ -83,15 +83,18 @@ def test_randomized_agreement_with_oracle(qs, orc, et):
         assert rel_fro(got, ref) <= tol, (Ma, Ka, Na, plan)
 
 
-def test_native_real_f64_bitwise_equals_scalar_kernel_order(qs, orc):
-    # The native FP64 kernel accumulates muladd(a, b, acc) ascending in the
+@pytest.mark.parametrize("tile", [1, 4])
+def test_native_simt_f64_bitwise_equals_scalar_kernel_order(qs, orc, tile):
+    # The SIMT gather kernel accumulates muladd(a, b, acc) ascending in the
     # plan's K order, like ScalarKernel: bitwise equal to the oracle.
     rng = np.random.default_rng(7)
     for (Ma, Ka, Na) in ((37, 29, 23), (130, 70, 65), (3072 // 16, 128, 80)):
         A = colmajor_pair(qs, rng, (Ma, Ka), "Float64")
         B = colmajor_pair(qs, rng, (Ka, Na), "Float64")
         C = colmajor_pair(qs, rng, (Ma, Na), "Float64")
-        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native")
+        got, ref, plan = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native",
+                                  native_tile=tile)
+        assert plan.native_tile == tile
         assert np.array_equal(got, ref)
 
 
@@ -99,18 +102,21 @@ def test_native_real_f64_bitwise_equals_scalar_kernel_order(qs, orc):
                                  (257, 300, 17)])
 @pytest.mark.parametrize("b_nfast", [False, True])
 def test_native_narrow_n_tiles_bitwise(qs, orc, MKN, b_nfast):
-    # The narrow-N tile shapes (256 x 16, 128 x 32) keep the ascending-K
+    # The SIMT narrow-N tile shapes (256 x 16, 128 x 32) keep the ascending-K
     # muladd order: bitwise equal to the oracle, for B stored K-fast or N-fast.
     Ma, Ka, Na = MKN
+    tile = 3 if Na <= 16 else 2 if Na <= 32 else 1
     rng = np.random.default_rng(Ma + Na)
     A = colmajor_pair(qs, rng, (Ma, Ka), "Float64")
     C = colmajor_pair(qs, rng, (Ma, Na), "Float64")
     if b_nfast:
         B = colmajor_pair(qs, rng, (Na, Ka), "Float64")
-        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (3, 2), 0.7, (1, 3), method="native")
+        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (3, 2), 0.7, (1, 3), method="native",
+                               native_tile=tile)
     else:
         B = colmajor_pair(qs, rng, (Ka, Na), "Float64")
-        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native")
+        got, ref, _ = run_pair(qs, orc, C, 1.3, A, (1, 2), B, (2, 3), 0.7, (1, 3), method="native",
+                               native_tile=tile)
     assert np.array_equal(got, ref)
 
 
@@ -131,15 +137,22 @@ def test_skinny_path(qs, orc, et, MKN):
         assert rel_fro(got, ref) <= 50 * K * eps(et)
 
 
-def test_small_problem_32x32_tiles_bitwise(qs, orc):
-    # The c0 permuted matmul (M = (a,b) = 96*32, N = 80, K = 128): a 64x64
-    # grid would leave SMs idle, so the plan takes 32x32 tiles; same FMA
-    # order, so bitwise equal to the oracle.
+def test_small_problem_tiles(qs, orc):
+    # The c0 permuted matmul (M = (a,b) = 96*32, N = 80, K = 128).  Real
+    # Float64 operands take the DMMA kernel; a 128x128 grid would leave SMs
+    # idle, so the plan takes 64x64 DMMA tiles.  The SIMT kernel's 32x32
+    # tiles (forced) keep the ScalarKernel FMA order: bitwise equal.
     rng = np.random.default_rng(96)
     A = colmajor_pair(qs, rng, (96, 128, 32), "Float64")
     B = colmajor_pair(qs, rng, (128, 80), "Float64")
     C = colmajor_pair(qs, rng, (96, 80, 32), "Float64")
+    C0 = C.host.parent.copy()
     got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2, 3), B, (2, 4), 0.0, (1, 4, 3))
+    assert plan.method == "native" and plan.native_tile == 4 + 2 + 1
+    assert rel_fro(got, ref) <= 50 * 128 * eps("Float64")
+    C.host.parent[:] = C0
+    C.dev.parent.copy_(torch.from_numpy(C0))
+    got, ref, plan = run_pair(qs, orc, C, 1.0, A, (1, 2, 3), B, (2, 4), 0.0, (1, 4, 3), native_tile=4)
     assert plan.method == "native" and plan.native_tile == 4
     assert np.array_equal(got, ref)
 
