@@ -78,6 +78,30 @@ def host_inputs(seed=20261203, wide=False):
     return A, B, C
 
 
+def c1_accuracy(orc, got, A_h, B_h, C_h):
+    """Relative Frobenius error of one execute's C (`got`, flat, from the
+    seeded C) over every element against the oracle's FP64 nest, and over a
+    sample of 8^4 elements spread over all four indices of C (every 8th
+    a, b, c, d) against the oracle in binary128."""
+    sa, sb, sc = shapes()
+    f64 = lambda x: np.ascontiguousarray(x, dtype=np.float64)  # noqa: E731
+    Ah = orc.HostView(f64(A_h), sa, colmajor_strides(sa))
+    Bh = orc.HostView(f64(B_h), sb, colmajor_strides(sb))
+    Cref = orc.HostView(f64(C_h).copy(), sc, colmajor_strides(sc))
+    orc.nest_f64(Cref, ALPHA, Ah, LABELS["indA"], Bh, LABELS["indB"], BETA, LABELS["indC"])
+    full = orc.rel_fro(got.astype(np.float64), Cref.parent)
+    picks = {1: (1, 8, 8), 2: (3, 8, 8), 3: (5, 8, 8), 4: (7, 8, 8)}
+    sub = lambda v, lab: orc.label_subview(v, lab, picks)  # noqa: E731
+    Cq = orc.HostView(f64(C_h).copy(), sc, colmajor_strides(sc))
+    Cs = sub(Cq, LABELS["indC"])
+    orc.brute(Cs, ALPHA, sub(Ah, LABELS["indA"]), LABELS["indA"], sub(Bh, LABELS["indB"]), LABELS["indB"], BETA,
+              LABELS["indC"], precision=1, threads=orc.max_threads())
+    gs = orc.HostView(got.astype(np.float64), Cs.size, Cs.strides, Cs.offset).to_array()
+    exact = orc.rel_fro(gs, Cs.to_array())
+    return {"rel_err": full, "elements": int(got.size), "rel_err_binary128": exact,
+            "sample": "every 8th index along each of a, b, c, d (4096 elements)"}
+
+
 def colmajor_strides(shape):
     st, acc = [], 1
     for s in shape:
@@ -274,12 +298,27 @@ def cpu_sample(orc, A, B, C, rows, threads):
     return 2.0 * rows * N * K / dt / 1e12, dt
 
 
+def host_cpu():
+    """The host's CPU model and logical core count (for the CPU baseline)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count()}
+
+
 def run_reference(args, rank, world):
-    """CPU arm: the oracle's nest restatement on all host threads, rank 0 only."""
+    """CPU arm: the oracle's nest restatement on all host threads (or
+    --cpu-threads), rank 0 only."""
     if rank != 0:
         return
     from oracle import oracle as orc
-    threads = orc.max_threads()
+    threads = args.cpu_threads or orc.max_threads()
     A, B, C = host_inputs()
     rows = args.cpu_rows
     for _ in range(args.warmup):
@@ -299,7 +338,7 @@ def run_reference(args, rank, world):
         "config": {"workload": WORKLOAD, "M": M, "N": N, "K": K, "alpha": ALPHA, "beta": BETA,
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "host": host_cpu()},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -789,6 +828,7 @@ def main():
                     help="Ozaki: the one-SM GEMM kernel instead of the CTA-pair (cta_group::2) kernel")
     ap.add_argument("--cpu-rows", type=int, default=M)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-threads", type=int, default=0, help="CPU arm threads (0: every host thread)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--profile", action="store_true",
@@ -867,20 +907,13 @@ def main():
     plan = qs.plan_contract(Cv, Av, LABELS["indA"], Bv, LABELS["indB"], LABELS["indC"], method=args.method,
                             per_product_gemm=args.per_product, oz_single_sm=args.oz_single_sm)
 
-    # Accuracy of the measured path: one execution from the seeded C against
-    # the FP64 oracle on a sample of C elements (first 2 rows of each 64-block
-    # of M... i.e. the leading elements of C in memory order).
+    # Accuracy of the measured path: one execution from the seeded C, every
+    # element against the FP64 oracle, and a binary128 sample spread over
+    # all of C (outside the timed region).
     from oracle import oracle as orc
     qs.execute(plan, ALPHA, BETA)
     torch.cuda.synchronize()
-    got = Cd.cpu().numpy()
-    nsamp = 8192
-    Cref = orc.HostView(C_h.astype(np.float64), sc, colmajor_strides(sc))
-    orc.brute(Cref, ALPHA, orc.HostView(A_h.astype(np.float64), sa, colmajor_strides(sa)), LABELS["indA"],
-              orc.HostView(B_h.astype(np.float64), sb, colmajor_strides(sb)), LABELS["indB"], BETA, LABELS["indC"],
-              c_range=(0, nsamp))
-    ref = Cref.parent[:nsamp]
-    rel_err = float(np.linalg.norm(got[:nsamp].astype(np.float64) - ref) / np.linalg.norm(ref))
+    acc = c1_accuracy(orc, Cd.cpu().numpy(), A_h, B_h, C_h)
 
     stream = torch.cuda.current_stream()
     # warm-up (untimed)
@@ -977,13 +1010,15 @@ def main():
         # Passes over args.cpu_rows rows of M until at least args.cpu_seconds
         # of CPU work (at most 16 passes); the median rate is reported.
         rates, total = [], 0.0
+        threads = args.cpu_threads or orc.max_threads()
         while total < args.cpu_seconds and len(rates) < 16:
-            v, dt = cpu_sample(orc, A_h, B_h, C_h, args.cpu_rows, orc.max_threads())
+            v, dt = cpu_sample(orc, A_h, B_h, C_h, args.cpu_rows, threads)
             rates.append(v)
             total += dt
-        cpu = {"value": statistics.median(rates), "unit": "TFLOP/s", "cores": orc.max_threads(), "kind": "port",
+        cpu = {"value": statistics.median(rates), "unit": "TFLOP/s", "cores": threads, "kind": "port",
                "sample": f"{len(rates)} passes of {args.cpu_rows} of {M} rows of M (all N, all K) through the "
-                         f"oracle's nest restatement, {total:.1f} s in total, median pass rate"}
+                         f"oracle's nest restatement, {total:.1f} s in total, median pass rate",
+               "host": host_cpu()}
 
     if rank == 0:
         print(json.dumps({
@@ -1000,7 +1035,8 @@ def main():
                        "dist": args.dist,
                        "l2": f"inputs larger than L2 ({419 if not f32 else 210} MB), no flush",
                        "parallelism": f"replicas{world}"},
-            "rel_err": rel_err, "rel_err_sample": nsamp,
+            "rel_err": acc["rel_err"], "rel_err_elements": acc["elements"],
+            "rel_err_binary128_sample": acc["rel_err_binary128"], "binary128_sample": acc["sample"],
             "roofline": roof, "stages_ms": stages,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,

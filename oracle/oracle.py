@@ -151,3 +151,29 @@ def nest_f64(C: HostView, alpha, A: HostView, indA, B: HostView, indB, beta, ind
 
 def max_threads() -> int:
     return lib().oracle_max_threads()
+
+
+def label_subview(v: HostView, labels, picks: dict) -> HostView:
+    """The sub-view of `v` (axes labelled `labels`) that keeps, for every
+    label in `picks` (label -> (start, step, count)), the indices start,
+    start + step, ..., start + (count - 1) * step of that label's axis.  A
+    contraction over such sub-views of A, B and C computes exactly the picked
+    elements of C: a sample spread over every index of C for the checker."""
+    size, strides, offset = list(v.size), list(v.strides), v.offset
+    for d, lab in enumerate(labels):
+        if lab in picks:
+            start, step, count = picks[lab]
+            assert 0 <= start and start + (count - 1) * step < size[d]
+            offset += start * strides[d]
+            strides[d] *= step
+            size[d] = count
+    return HostView(v.parent, size, strides, offset, v.op)
+
+
+def rel_fro(got: np.ndarray, ref: np.ndarray) -> float:
+    """Relative Frobenius error ||got - ref|| / ||ref||, accumulated in
+    extended precision."""
+    ref = np.asarray(ref, dtype=np.complex256 if np.iscomplexobj(ref) else np.longdouble)
+    d = np.linalg.norm((np.asarray(got, dtype=ref.dtype) - ref).ravel())
+    n = np.linalg.norm(ref.ravel())
+    return float(d / n) if n > 0 else float(d)
