@@ -73,7 +73,6 @@ struct Workspace {
   int32_t *expA = nullptr;  // per packed row of A (Ozaki), or nullptr
   int32_t *expB = nullptr;
   int32_t *status = nullptr;  // device status word (bounded waits)
-  void *rowmax = nullptr;     // Ozaki: per-row max |x| bit patterns
   size_t bytes = 0;
   std::vector<void *> owned;         // every allocated block, for freeing
   std::vector<size_t> owned_bytes;   // and its size (for a qs_allocator)

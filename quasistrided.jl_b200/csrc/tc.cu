@@ -163,84 +163,12 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
   }
 }
 
-// Ozaki pass 1: each row's max magnitude, as the bit pattern of |x| (for
-// non-negative doubles the integer order is the value order, and any NaN or
-// Inf sorts above every finite value).  Grid: 32-row blocks x 128-wide K
-// blocks; one atomicMax per row and block.
-__device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, unsigned long long *rowmax,
-                                                int64_t r0, int64_t k0) {
-  __shared__ double tile[32][129];
-  load_tile<double, 128>(a, r0, k0, tile);
-  __syncthreads();
-  const int row = threadIdx.x >> 3, part = threadIdx.x & 7;  // 8 threads per row
-  unsigned long long m = 0;
-#pragma unroll
-  for (int kk = 0; kk < 16; ++kk) {
-    unsigned long long b = (unsigned long long)__double_as_longlong(fabs(tile[row][tcol<128>(part * 16 + kk)]));
-    m = b > m ? b : m;
-  }
-#pragma unroll
-  for (int o = 1; o < 8; o <<= 1) {
-    unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
-    m = x > m ? x : m;
-  }
-  if (part == 0 && r0 + row < a.rows && m) atomicMax(rowmax + r0 + row, m);
-}
-
-// Ozaki pass 2: the digit planes of one 32-row x 128-byte block.  With
-// E = (frexp exponent of the row max) + 1, x = v * 2^-E has |x| < 1/2, and
+// Ozaki digits of a row (the fused pack below): with E = (frexp exponent of
+// the row's max |x|) + 1, x = v * 2^-E has |x| < 1/2, and
 //   for p = 1..s: y = 254 x; d_p = rint(y); x = y - d_p
 // gives digits |d_p| <= 127 with v ~= 2^E * sum_p d_p 254^-p; the error is
 // the tail 254^-s plus one rounding of 254 x per digit.  Rows with a NaN or
 // Inf get exponent kNonFinite, zero digits, and are listed for the fixup.
-__device__ __forceinline__ void oz_slice_block(const PackArgs &a, const unsigned long long *rowmax,
-                                               int64_t r0, int64_t k0) {
-  __shared__ double tile[32][129];
-  load_tile<double, 128>(a, r0, k0, tile);
-  __syncthreads();
-  const int row = threadIdx.x >> 3, c = threadIdx.x & 7;  // 16-byte chunk c of the row
-  const int64_t grow = r0 + row;
-  if (grow >= a.rows_pad) return;
-  const unsigned long long mb = grow < a.rows ? rowmax[grow] : 0ull;
-  int E = 0;
-  const bool bad = mb >= 0x7FF0000000000000ull;
-  if (bad) {
-    E = kNonFinite;
-  } else if (mb) {
-    frexp(__longlong_as_double((long long)mb), &E);
-    E += 1;
-  }
-  if (k0 == 0 && c == 0) {
-    a.exp_out[grow] = E;
-    if (bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
-  }
-  double x[16];
-#pragma unroll
-  for (int kk = 0; kk < 16; ++kk) {
-    const double v = tile[row][tcol<128>(c * 16 + kk)];
-    x[kk] = (bad || !mb) ? 0.0 : scale2(v, -E);
-  }
-  const int64_t off = panel_tile_base(a, grow, k0 + c * 16);
-  for (int p = 0; p < a.nslices; ++p) {
-    uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      // y = 254 x; d = y rounded to the nearest integer (ties to even, like
-      // rint) by adding and removing 1.5 * 2^52, whose low word then holds
-      // d in two's complement; x = y - d.  Four full-rate FP64 adds and
-      // multiplies, no rounding or conversion instructions; the _rn
-      // intrinsics keep the compiler from fusing the steps.
-      constexpr double kRound = 6755399441055744.0;
-      const double y = __dmul_rn(x[kk], 254.0);
-      const double t = __dadd_rn(y, kRound);
-      const double d = __dsub_rn(t, kRound);
-      x[kk] = __dsub_rn(y, d);
-      const uint32_t byte = (uint32_t)__double2loint(t) & 0xFFu;
-      w[kk >> 2] |= byte << (8 * (kk & 3));
-    }
-    *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-}
 
 // Split-BF16 planes of one 32-row x 64-element block: hi = bf16(x),
 // lo = bf16(x - hi), x in FP32.
@@ -274,32 +202,6 @@ __device__ __forceinline__ void split_block(int64_t b, int nrb, int64_t &r0, int
   r0 = (b % nrb) * 32;
   kb = b / nrb;
 }
-__global__ void __launch_bounds__(256, 6)  // six 33 KB tiles per SM, as one operand per launch had
-    oz_rowmax_pair_kernel(PackArgs pa, PackArgs pb, unsigned long long *rma, unsigned long long *rmb, int nrbA,
-                          int nrbB, int64_t nA) {
-  int64_t r0, kb;
-  const int64_t b = blockIdx.x;
-  if (b < nA) {
-    split_block(b, nrbA, r0, kb);
-    oz_rowmax_block(pa, rma, r0, kb * 128);
-  } else {
-    split_block(b - nA, nrbB, r0, kb);
-    oz_rowmax_block(pb, rmb, r0, kb * 128);
-  }
-}
-__global__ void __launch_bounds__(256)
-    oz_slice_pair_kernel(PackArgs pa, PackArgs pb, const unsigned long long *rma, const unsigned long long *rmb,
-                         int nrbA, int nrbB, int64_t nA) {
-  int64_t r0, kb;
-  const int64_t b = blockIdx.x;
-  if (b < nA) {
-    split_block(b, nrbA, r0, kb);
-    oz_slice_block(pa, rma, r0, kb * 128);
-  } else {
-    split_block(b - nA, nrbB, r0, kb);
-    oz_slice_block(pb, rmb, r0, kb * 128);
-  }
-}
 __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackArgs pb, int nrbA, int nrbB,
                                                              int64_t nA) {
   int64_t r0, kb;
@@ -310,6 +212,163 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
   } else {
     split_block(b - nA, nrbB, r0, kb);
     bf16_pack_block(pb, r0, kb * 64);
+  }
+}
+
+// Fused Ozaki pack: both passes in one launch, each operand read once from
+// HBM.  A CTA walks bands of kBandRows rows of one operand (A's bands, then
+// B's).  Phase 1 streams the band's K tiles and reduces every row's max
+// |x| bit pattern in registers (no atomics, nothing to clear per execute);
+// phase 2 streams the band again and emits the digit planes.  The grid is a
+// few CTAs per SM, so the bands in flight (kBandRows * K * 8 bytes each)
+// stay in L2 between the two phases and phase 2 reads them from there.
+constexpr int kBandRows = 8, kBandK = 512;
+constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 double per 16, +4 per row: conflict-free
+
+__device__ __forceinline__ int band_col(int k) { return k + (k >> 4); }
+
+// K tile [k0, k0 + kBandK) of rows [r0, r0 + kBandRows) into `tile`
+// (virtual matrix values, zero outside rows/K), coalesced along X's
+// unit-stride axis.  STREAM: the band's second read (L2, evict first).
+template <bool STREAM>
+__device__ __forceinline__ void load_band(const PackArgs &a, int64_t r0, int64_t k0,
+                                          double (*tile)[kBandStride]) {
+  const int tid = threadIdx.x;
+  constexpr int PER = kBandRows * kBandK / 256;
+  if (a.cmode == 0 && (a.TX == QS_F64 || a.TX == QS_F32)) {
+    const bool f64 = a.TX == QS_F64;
+    auto ld = [&](int64_t idx) -> double {
+      if (f64) {
+        const double *p = static_cast<const double *>(a.X) + idx;
+        return STREAM ? __ldcs(p) : __ldg(p);
+      }
+      const float *p = static_cast<const float *>(a.X) + idx;
+      return (double)(STREAM ? __ldcs(p) : __ldg(p));
+    };
+    if (a.rfast) {
+      const int rr = tid % kBandRows, kb = tid / kBandRows;
+      const int64_t r = r0 + rr;
+      const bool rok = r < a.rows;
+      const int64_t ro = rok ? a.Xbase + __ldg(a.offR + r) : 0;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int kk = kb + (256 / kBandRows) * i;
+        const int64_t k = k0 + kk;
+        const bool ok = rok && k < a.K;
+        tile[rr][band_col(kk)] = ok ? ld(ro + __ldg(a.offK + k)) : 0.0;
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < kBandK / 256; ++h) {
+        const int kk = tid + 256 * h;
+        const int64_t k = k0 + kk;
+        const bool kok = k < a.K;
+        const int64_t ko = kok ? a.Xbase + __ldg(a.offK + k) : 0;
+#pragma unroll
+        for (int rr = 0; rr < kBandRows; ++rr) {
+          const int64_t r = r0 + rr;
+          const bool ok = kok && r < a.rows;
+          tile[rr][band_col(kk)] = ok ? ld(ko + __ldg(a.offR + r)) : 0.0;
+        }
+      }
+    }
+    return;
+  }
+#pragma unroll 4
+  for (int i = 0; i < PER; ++i) {
+    int rr, kk;
+    if (a.rfast) {
+      rr = tid % kBandRows;
+      kk = tid / kBandRows + (256 / kBandRows) * i;
+    } else {
+      kk = tid + 256 * (i % (kBandK / 256));
+      rr = i / (kBandK / 256);
+    }
+    const int64_t r = r0 + rr, k = k0 + kk;
+    tile[rr][band_col(kk)] = (r < a.rows && k < a.K) ? virtual_elem<double>(a, r, k) : 0.0;
+  }
+}
+
+// One band: warp w owns row r0 + w, lane l its K values 16 l .. 16 l + 15 of
+// each K tile.
+__device__ __forceinline__ void oz_pack_band(const PackArgs &a, int64_t r0, double (*tile)[kBandStride]) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t grow = r0 + w;
+  const int64_t kpad = (int64_t)a.kblocks * kKBytes;  // digits written per row (bytes = K values)
+  unsigned long long mb = 0;
+  for (int64_t k0 = 0; k0 < a.K; k0 += kBandK) {
+    load_band<false>(a, r0, k0, tile);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      const unsigned long long b =
+          (unsigned long long)__double_as_longlong(fabs(tile[w][band_col(lane * 16 + kk)]));
+      mb = b > mb ? b : mb;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, mb, o);
+    mb = x > mb ? x : mb;
+  }
+  // E: the row max's frexp exponent + 1; non-finite rows get kNonFinite,
+  // zero digits and a place on the fixup list.
+  int E = 0;
+  const bool bad = mb >= 0x7FF0000000000000ull;
+  if (bad) {
+    E = kNonFinite;
+  } else if (mb) {
+    frexp(__longlong_as_double((long long)mb), &E);
+    E += 1;
+  }
+  const bool live = grow < a.rows_pad;
+  if (live && lane == 0) {
+    a.exp_out[grow] = E;
+    if (bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
+  }
+  for (int64_t k0 = 0; k0 < kpad; k0 += kBandK) {
+    if (k0 < a.K) load_band<true>(a, r0, k0, tile);
+    __syncthreads();
+    const int64_t kc = k0 + lane * 16;
+    if (live && kc < kpad) {
+      double x[16];
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk) {
+        const double v = k0 < a.K ? tile[w][band_col(lane * 16 + kk)] : 0.0;
+        x[kk] = (bad || !mb) ? 0.0 : scale2(v, -E);
+      }
+      const int64_t off = panel_tile_base(a, grow, kc);
+      for (int p = 0; p < a.nslices; ++p) {
+        uint32_t wd[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+          // y = 254 x; d = y rounded to the nearest integer (ties to even, like
+          // rint) by adding and removing 1.5 * 2^52, whose low word then holds
+          // d in two's complement; x = y - d.  Four full-rate FP64 adds and
+          // multiplies, no rounding or conversion instructions; the _rn
+          // intrinsics keep the compiler from fusing the steps.
+          constexpr double kRound = 6755399441055744.0;
+          const double y = __dmul_rn(x[kk], 254.0);
+          const double t = __dadd_rn(y, kRound);
+          const double d = __dsub_rn(t, kRound);
+          x[kk] = __dsub_rn(y, d);
+          wd[kk >> 2] |= ((uint32_t)__double2loint(t) & 0xFFu) << (8 * (kk & 3));
+        }
+        *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Both operands of one plan: bands [0, nbA) of A, then [0, nbB) of B.
+__global__ void __launch_bounds__(256, 2)
+    oz_pack_fused_kernel(PackArgs pa, PackArgs pb, int64_t nbA, int64_t nbB) {
+  __shared__ double tile[kBandRows][kBandStride];
+  for (int64_t b = blockIdx.x; b < nbA + nbB; b += gridDim.x) {
+    if (b < nbA) oz_pack_band(pa, b * kBandRows, tile);
+    else oz_pack_band(pb, (b - nbA) * kBandRows, tile);
   }
 }
 
@@ -1401,9 +1460,6 @@ int tc_prepare(qs_plan *p) {
     p->ws.expB = b + g.Mp;
     if (setup_zero_async(q, n * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
     p->ws.status = b + n - 1;
-    // row/column max bit patterns, cleared per execute
-    if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
-    p->ws.rowmax = q;
   } else {
     if ((rc = tc_alloc(p, &q, 4 * sizeof(int32_t)))) return rc;
     if (setup_zero_async(q, 4 * sizeof(int32_t)) != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
@@ -1604,23 +1660,21 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
   if (ev) cudaEventRecord(ev[0], st);
-  if (oz) {
-    e = cudaMemsetAsync(p->ws.rowmax, 0, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long), st);
-    if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
-  }
   {
-    // Both operands per launch.  Profile stages: Ozaki ev[1] after the
-    // row-max pass, ev[2] after the digit planes; BF16x3 both after the pack.
+    // Both operands per launch.  Profile stages: ev[1] and ev[2] both after
+    // the pack (Ozaki: the fused row-max + digit-plane kernel).
     const PackArgs pa = pack_args(p, 0), pb = pack_args(p, 1);
     const int nrbA = (int)cdiv(pa.rows_pad, 32), nrbB = (int)cdiv(pb.rows_pad, 32);
     const int64_t nA = (int64_t)nrbA * g.kblocks, nB = (int64_t)nrbB * g.kblocks;
     if (oz) {
-      unsigned long long *rma = (unsigned long long *)p->ws.rowmax, *rmb = rma + g.Mp;
-      oz_rowmax_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, rma, rmb, nrbA, nrbB, nA);
-      if (ev) cudaEventRecord(ev[1], st);
-      oz_slice_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, rma, rmb, nrbA, nrbB, nA);
-      if (ev) cudaEventRecord(ev[2], st);
-      launches += 2;
+      const int64_t nbA = cdiv(pa.rows_pad, kBandRows), nbB = cdiv(pb.rows_pad, kBandRows);
+      const int grid = (int)std::min<int64_t>(nbA + nbB, 2 * (int64_t)num_sms());
+      oz_pack_fused_kernel<<<grid, 256, 0, st>>>(pa, pb, nbA, nbB);
+      if (ev) {
+        cudaEventRecord(ev[1], st);
+        cudaEventRecord(ev[2], st);
+      }
+      ++launches;
     } else {
       bf16_pack_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, nrbA, nrbB, nA);
       if (ev) {
@@ -1674,24 +1728,23 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
 }
 
 // ---------------------------------------------------------- grouped ---
-// Many independent plans of one class as one launch per stage: pack (rowmax
+// Many independent plans of one class as one launch per stage: pack (fused
 // and slices, or the BF16 planes), the persistent GEMM over a problem table,
 // and the non-finite fixup.  Each plan keeps its own workspace; the launch
 // reads per-problem arguments from device tables.
 
 // One operand side of one problem in a grouped pack launch: blocks
 // [block_start, block_start + gx * kblocks) of the launch.
+// Ozaki: blocks are kBandRows-row bands (gx of them); BF16x3: 32-row x 64-K
+// blocks (gx row blocks x kblocks).
 struct PackJob {
   PackArgs pa;
-  unsigned long long *rowmax;  // Ozaki: this side's row-max words
-  int gx;                      // 32-row blocks
+  int gx;
   int block_start;
 };
 
-// A per-plan prep: the row-max words and the non-finite counters to zero.
+// A per-plan prep: the non-finite counters to zero.
 struct ZeroJob {
-  unsigned long long *rowmax;
-  int64_t nwords;  // even: Mp + Np
   int32_t *counters;
 };
 
@@ -1706,26 +1759,18 @@ __device__ __forceinline__ int pack_job(const PackJob *jobs, int njobs, int b) {
 }
 
 __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int n) {
-  for (int j = blockIdx.x; j < n; j += gridDim.x) {
-    const ZeroJob z = jobs[j];
-    uint4 *w = reinterpret_cast<uint4 *>(z.rowmax);
-    for (int64_t i = threadIdx.x; i < z.nwords / 2; i += blockDim.x) w[i] = make_uint4(0, 0, 0, 0);
-    if (threadIdx.x < 2) z.counters[threadIdx.x] = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += gridDim.x * blockDim.x)
+    jobs[j >> 1].counters[j & 1] = 0;
+}
+
+// The fused pack over every band of every (problem, side) job.
+__global__ void __launch_bounds__(256, 2) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
+  __shared__ double tile[kBandRows][kBandStride];
+  for (int b = blockIdx.x; b < nbands; b += gridDim.x) {
+    const PackJob &j = jobs[pack_job(jobs, njobs, b)];
+    const PackArgs pa = j.pa;
+    oz_pack_band(pa, (int64_t)(b - j.block_start) * kBandRows, tile);
   }
-}
-
-__global__ void __launch_bounds__(256) oz_rowmax_grouped(const PackJob *jobs, int njobs) {
-  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
-  const int lb = blockIdx.x - j.block_start;
-  const PackArgs pa = j.pa;
-  oz_rowmax_block(pa, j.rowmax, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 128);
-}
-
-__global__ void __launch_bounds__(256) oz_slice_grouped(const PackJob *jobs, int njobs) {
-  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
-  const int lb = blockIdx.x - j.block_start;
-  const PackArgs pa = j.pa;
-  oz_slice_block(pa, j.rowmax, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 128);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
@@ -1772,10 +1817,9 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
     for (int side = 0; side < 2; ++side) {
       PackJob j;
       j.pa = pack_args(p, side);
-      j.rowmax = oz ? (unsigned long long *)p->ws.rowmax + (side ? tg.Mp : 0) : nullptr;
-      j.gx = (int)cdiv(j.pa.rows_pad, 32);
+      j.gx = (int)cdiv(j.pa.rows_pad, oz ? kBandRows : 32);
       j.block_start = blocks;
-      const int64_t nb = (int64_t)j.gx * tg.kblocks;
+      const int64_t nb = oz ? (int64_t)j.gx : (int64_t)j.gx * tg.kblocks;
       if (blocks + nb > INT_MAX) return fail(QS_EINVAL, "ArgumentError: grouped pack launch too large");
       blocks += (int)nb;
       jobs.push_back(j);
@@ -1786,8 +1830,6 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
     tiles.push_back((int)t);
     if (oz) {
       ZeroJob z;
-      z.rowmax = (unsigned long long *)p->ws.rowmax;
-      z.nwords = tg.Mp + tg.Np;
       z.counters = p->ws.expA + tg.Mp + tg.Np + tg.Mp + tg.Np;
       zero.push_back(z);
       fix.push_back(make_fixup_job(p, al, be, bcase[g.idx[i]]));
@@ -1858,9 +1900,8 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const ZeroJob *zero = (const ZeroJob *)(d + g.off_zero);
     const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
     const int pgrid = std::min(n, 4 * num_sms());
-    oz_prep_grouped<<<pgrid, 256, 0, st>>>(zero, n);
-    oz_rowmax_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
-    oz_slice_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
+    oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
+    oz_pack_fused_grouped<<<std::min(g.pack_blocks, 2 * num_sms()), 256, 0, st>>>(jobs, g.njobs, g.pack_blocks);
     if (g.cls == TC_CLASS_OZ4)
       oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
     else if (g.cls == TC_CLASS_OZ6)
@@ -1870,7 +1911,7 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     else
       tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(base, gt);
     oz_fixup_grouped<<<pgrid, 256, 0, st>>>(fix, n);
-    l = 5;
+    l = 4;  // prep, fused pack, GEMM, fixup
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
