@@ -1729,7 +1729,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
 
 // ---------------------------------------------------------- grouped ---
 // Many independent plans of one class as one launch per stage: pack (fused
-// and slices, or the BF16 planes), the persistent GEMM over a problem table,
+// row-max and digit planes, or the BF16 planes), the persistent GEMM over a problem table,
 // and the non-finite fixup.  Each plan keeps its own workspace; the launch
 // reads per-problem arguments from device tables.
 
