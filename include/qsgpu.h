@@ -330,6 +330,19 @@ int qs_plan_stage_times(qs_plan *plan, double *stage_ms, int32_t max_stages,
  * the last check, else QS_OK. */
 int qs_plan_check_status(qs_plan *plan, void *stream);
 
+/* Failure detection (no counterpart in the reference, whose engine has no
+ * device waits).  Every barrier wait of the plan's tensor-core kernels gives
+ * up after `limit_ns` (0: the default, 2 s); the kernel then stops without
+ * writing C, waits (with the same bound) for the copies and MMAs it already
+ * issued, releases its tensor memory and returns, and qs_plan_check_status
+ * reports QS_ETIMEOUT; the GPU and the plan stay usable.  `hold_loads` != 0
+ * makes the GEMM's producers issue no operand copies at all, so the first
+ * wait for an operand tile runs out with nothing in flight: a way for tests
+ * to exercise that error path without a fault.  A captured graph of the plan
+ * (QS_PLAN_CUDA_GRAPH) is re-captured at the next execute.  Limits above
+ * 60 s are QS_EINVAL. */
+int qs_plan_set_wait_limit(qs_plan *plan, uint64_t limit_ns, int32_t hold_loads);
+
 /* Device arena: the device counterpart of TensorOperations' BufferAllocator
  * (the allocators plan_contract accepts; checkpoint/reset bracket every
  * TO.tensorcontract!, src/integrations/tensoroperations.jl:84-86).  A bump

@@ -32,16 +32,16 @@ import torch
 from . import _abi
 from .allocators import (DeviceArena, TorchAllocator, allocator_checkpoint,  # noqa: F401
                          allocator_handle, allocator_reset, tensoralloc, tensorfree)
-from ._abi import (ArgumentError, BoundsError, DimensionMismatch, EngineError,  # noqa: F401
-                   QS_C32, QS_C64, QS_F32, QS_F64)
+from ._abi import (ArgumentError, BoundsError, DeviceTimeout, DimensionMismatch,  # noqa: F401
+                   EngineError, QS_C32, QS_C64, QS_F32, QS_F64)
 
 __all__ = [
     "StridedView", "plan_contract", "execute", "contract", "ContractPlan", "PathModes",
     "QuasiStridedBackend", "tensorcontract", "contraction_labels", "release",
-    "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "colmajor",
+    "ArgumentError", "DimensionMismatch", "BoundsError", "EngineError", "DeviceTimeout", "colmajor",
     "execute_grouped", "ContractGroup", "add_trace", "tensoradd", "tensortrace",
     "DeviceArena", "TorchAllocator", "tensoralloc", "tensorfree", "allocator_checkpoint",
-    "allocator_reset",
+    "allocator_reset", "check_status", "set_wait_limit",
 ]
 
 _DTYPE_TO_QS = {torch.float32: QS_F32, torch.float64: QS_F64,
@@ -388,6 +388,15 @@ def check_status(plan: ContractPlan, stream=None) -> None:
     """Raise EngineError if a tensor-core kernel of this plan gave up a
     bounded wait since the last check (synchronizes the stream)."""
     _abi.check(_abi.lib().qs_plan_check_status(plan._h, _stream_ptr(stream)))
+
+
+def set_wait_limit(plan: ContractPlan, limit_ns: int = 0, hold_loads: bool = False) -> None:
+    """Bound every device wait of the plan's tensor-core kernels by `limit_ns`
+    (0: the default 2 s).  `hold_loads` is for failure-detection tests: the
+    GEMM's producers issue no copies, so the first wait for operand tiles
+    runs out and the kernel stops with QS_ETIMEOUT (nothing in flight, C
+    untouched).  qs_plan_set_wait_limit."""
+    _abi.check(_abi.lib().qs_plan_set_wait_limit(plan._h, int(limit_ns), int(bool(hold_loads))))
 
 
 def release(plan: ContractPlan, allocator=None) -> None:

@@ -39,6 +39,11 @@ class EngineError(RuntimeError):
     """A device-side failure (CUDA error, allocation failure, timeout)."""
 
 
+class DeviceTimeout(EngineError):
+    """A bounded device wait of a tensor-core kernel gave up (QS_ETIMEOUT):
+    the kernel stopped without writing C; the GPU and the plan stay usable."""
+
+
 class qs_view(ctypes.Structure):
     _fields_ = [
         ("data", ctypes.c_void_p),
@@ -157,6 +162,7 @@ SIGNATURES = {
     "qs_plan_stage_times": (ctypes.c_int, [_P, _DP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
     "qs_plan_check_status": (ctypes.c_int, [_P, _P]),
+    "qs_plan_set_wait_limit": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int32]),
     "qs_contract_noalloc": (ctypes.c_int, [ctypes.POINTER(qs_view), _DP, ctypes.POINTER(qs_view), _I64P,
                                            ctypes.POINTER(qs_view), _I64P, _DP, _I64P,
                                            ctypes.POINTER(qs_plan_options), _P]),
@@ -209,4 +215,6 @@ def check(rc: int) -> None:
         raise DimensionMismatch(msg)
     if rc == QS_EBOUNDS:
         raise BoundsError(msg)
+    if rc == QS_ETIMEOUT:
+        raise DeviceTimeout(f"status {rc}: {msg}")
     raise EngineError(f"status {rc}: {msg}")

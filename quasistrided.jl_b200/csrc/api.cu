@@ -397,6 +397,7 @@ size_t qs_last_error(char *buf, size_t n);  // defined below
 int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const int64_t *indA,
                      const qs_view *B, const int64_t *indB, const int64_t *indC,
                      const qs_plan_options *opts) {
+  qs::NvtxRange nvtx("qs_plan_contract");
   if (!out) return fail(QS_EINVAL, "ArgumentError: plan output pointer is NULL");
   *out = nullptr;
   qs_plan *p = new (std::nothrow) qs_plan();
@@ -464,6 +465,7 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
 }
 
 int qs_execute(qs_plan *p, const double *alpha, const double *beta, void *stream) {
+  qs::NvtxRange nvtx("qs_execute");
   if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
   if (!alpha || !beta) return fail(QS_EINVAL, "ArgumentError: alpha/beta is NULL");
   if (p->host_only)
@@ -597,6 +599,16 @@ int qs_plan_check_status(qs_plan *p, void *stream) {
   return QS_OK;
 }
 
+int qs_plan_set_wait_limit(qs_plan *p, uint64_t limit_ns, int32_t hold_loads) {
+  if (!p) return fail(QS_EINVAL, "ArgumentError: plan is NULL");
+  if (limit_ns > 60000000000ull)
+    return fail(QS_EINVAL, "ArgumentError: a wait limit above 60 s is not a bound");
+  p->wait_ns = limit_ns ? limit_ns : 2000000000ull;
+  p->hold_loads = hold_loads ? 1 : 0;
+  if (!p->host_only) destroy_graph(p);  // a captured graph holds the old arguments
+  return QS_OK;
+}
+
 int qs_plan_destroy(qs_plan *p) {
   if (!p) return QS_OK;
   if (!p->host_only) {
@@ -620,6 +632,7 @@ int qs_plan_destroy(qs_plan *p) {
 int qs_contract(const qs_view *C, const double *alpha, const qs_view *A, const int64_t *indA,
                 const qs_view *B, const int64_t *indB, const double *beta, const int64_t *indC,
                 const qs_plan_options *opts, void *stream) {
+  qs::NvtxRange nvtx("qs_contract");
   qs_plan_options o{};
   if (opts) o = *opts;
   o.flags &= ~QS_PLAN_HOST_ONLY;

@@ -295,6 +295,7 @@ int qs_group_create(int32_t n, qs_plan *const *plans, int32_t mode, qs_group **o
 }
 
 int qs_group_execute(qs_group *g, const double *alpha, const double *beta, void *stream) {
+  qs::NvtxRange nvtx("qs_group_execute");
   if (!g) return fail(QS_EINVAL, "ArgumentError: group is NULL");
   const int n = (int)g->plans.size();
   if (n == 0) return QS_OK;

@@ -69,6 +69,7 @@ struct Oz2MmaCtx {
   uint64_t *fullA, *emptyA, *fullB, *emptyB;
   volatile int *abort;
   int *status;
+  uint64_t limit;  // wait bound (ns)
 };
 
 // Release load L's slot if step ST is its last use (compile-time choice).
@@ -100,8 +101,8 @@ __device__ __forceinline__ bool oz2_mma_step(Oz2MmaCtx &c) {
   uint32_t sla, pa, slb, pb;
   ring_slot<kOzRingA>(c.r.a0, c.r.pa, oa, sla, pa);
   ring_slot<kOzRingB>(c.r.b0, c.r.pb, ob, slb, pb);
-  if (wait_a && !mbar_wait(&c.fullA[sla], pa, c.abort, c.status, QS_ETIMEOUT)) return false;
-  if (wait_b && !mbar_wait(&c.fullB[slb], pb, c.abort, c.status, QS_ETIMEOUT)) return false;
+  if (wait_a && !mbar_wait(&c.fullA[sla], pa, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
+  if (wait_b && !mbar_wait(&c.fullB[slb], pb, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
   if (wait_a || wait_b) tc_fence_after();
   const uint32_t d = c.tmem + acc * 128;
   const uint64_t adesc = sw128_kmajor_desc(c.slotsA_u32 + sla * 16384u);
@@ -130,6 +131,8 @@ struct Oz2LoadCtx {
   uint32_t rank;
   volatile int *abort;
   int *status;
+  uint64_t limit;            // wait bound (ns)
+  uint32_t issuedA, issuedB;  // fills issued per ring, in ring order (the exit drain's counts)
 };
 
 template <int S, int GI, int LD>
@@ -142,13 +145,16 @@ __device__ __forceinline__ bool oz2_load(Oz2LoadCtx &c) {
   else ring_slot<kOzRingB>(c.r.b0, c.r.pb, ord, slot, par);
   uint64_t *full = side == 0 ? &c.fullA[slot] : &c.fullB[slot];
   uint64_t *empty = side == 0 ? &c.emptyA[slot] : &c.emptyB[slot];
-  if (!mbar_wait(empty, par ^ 1u, c.abort, c.status, QS_ETIMEOUT)) return false;
+  if (!mbar_wait(empty, par ^ 1u, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
   if (c.rank == 0) mbar_arrive_expect_tx(full, 2 * BYTES);
   const uint32_t mbar = mapa_u32(full, 0);
-  if (side == 0)
+  if (side == 0) {
     tma_load_2d_pair(c.slotsA + slot * 16384u, c.tmA, 0, c.yA + slice * c.planeRowsA, mbar);
-  else
+    ++c.issuedA;
+  } else {
     tma_load_2d_pair(c.slotsB + slot * kOzHalfB, c.tmB, 0, c.yB + slice * c.planeRowsB, mbar);
+    ++c.issuedB;
+  }
   return true;
 }
 
@@ -185,7 +191,7 @@ __device__ __forceinline__ bool oz2_mma_group(const GemmArgs &a, uint32_t &LA, u
   for (int ks = 0; ks < a.nkseg; ++ks) {
 #pragma unroll
     for (int q = 0; q < NACC; ++q)
-      if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, c.abort, c.status, QS_ETIMEOUT))
+      if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, c.abort, c.status, QS_ETIMEOUT, c.limit))
         return false;
     tc_fence_after();
     c.started = 0;
@@ -214,7 +220,7 @@ __device__ __forceinline__ bool oz2_drain_group(const GemmArgs &a, uint32_t &acc
   for (int ks = 0; ks < a.nkseg; ++ks) {
 #pragma unroll
     for (int qa = 0; qa < NACC; ++qa) {
-      if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT)) return false;
+      if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT, a.wait_ns)) return false;
       tc_fence_after();
       const double w = a.wdiag[T0 + qa];
 #pragma unroll
@@ -237,6 +243,35 @@ __device__ __forceinline__ bool oz2_drain_group(const GemmArgs &a, uint32_t &acc
     }
   }
   return true;
+}
+
+// The even CTA's exit drain of one ring: every fill either CTA issued has
+// landed.  Both CTAs' copies complete on the even CTA's full barriers, which
+// the even producer arms for both halves, so per slot the two CTAs can be
+// one fill apart when a wait gave up (a CTA refills a slot only after the
+// MMA consumed the slot's previous fill, which needed both halves):
+//  - the odd CTA one fill ahead: arm that phase for the odd half alone;
+//  - this CTA one fill ahead: count the missing odd half as done;
+// then wait for the slot's last phase.  issuedE / issuedO: the CTAs' fills
+// in ring order; half: the bytes of one CTA's half of a fill.
+__device__ __forceinline__ void oz2_drain_ring(uint64_t *full, int nslots, uint32_t issuedE, uint32_t issuedO,
+                                               uint32_t half, int *status, uint64_t limit) {
+  for (int s = 0; s < nslots; ++s) {
+    const int fE = issuedE > (uint32_t)s ? (int)((issuedE - 1u - (uint32_t)s) / (uint32_t)nslots) : -1;
+    const int fO = issuedO > (uint32_t)s ? (int)((issuedO - 1u - (uint32_t)s) / (uint32_t)nslots) : -1;
+    if (fE < 0 && fO < 0) continue;
+    if (fO == fE + 1) {
+      if (fE >= 0 && !mbar_wait_drain(&full[s], (uint32_t)fE & 1u, status, limit)) continue;
+      mbar_arrive_expect_tx(&full[s], half);
+      mbar_wait_drain(&full[s], (uint32_t)fO & 1u, status, limit);
+    } else if (fE == fO + 1) {
+      if (fO >= 0 && !mbar_wait_drain(&full[s], (uint32_t)fO & 1u, status, limit)) continue;
+      mbar_complete_tx(&full[s], half);
+      mbar_wait_drain(&full[s], (uint32_t)fE & 1u, status, limit);
+    } else {
+      mbar_wait_drain(&full[s], (uint32_t)(fE > fO ? fE : fO) & 1u, status, limit);
+    }
+  }
 }
 
 // Pair tile t -> (m-pair, n-tile), in bands of kBandM / 2 m-pairs: the same
@@ -265,8 +300,10 @@ __global__ void __launch_bounds__(320, 1)
   uint64_t *bars = (uint64_t *)(smem + kOzSlots * TILE);
   uint64_t *fullA = bars, *emptyA = fullA + kOzRingA, *fullB = emptyA + kOzRingA, *emptyB = fullB + kOzRingB;
   uint64_t *accf = emptyB + kOzRingB, *acce = accf + 4;
-  uint32_t *tmem_slot = (uint32_t *)(acce + 4);
+  uint64_t *drainb = acce + 4;  // the MMA's exit drain (committed to both CTAs)
+  uint32_t *tmem_slot = (uint32_t *)(drainb + 1);
   volatile int *abort = (volatile int *)(tmem_slot + 1);
+  uint32_t *s_issued = (uint32_t *)(tmem_slot + 2);  // [A, B] of the even CTA, [A, B] of the odd CTA
   int64_t *s_offN = (int64_t *)(smem + kOzSlots * TILE + 1024);
   int32_t *s_expN = (int32_t *)(s_offN + 128);
 
@@ -285,7 +322,9 @@ __global__ void __launch_bounds__(320, 1)
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 16);
     }
+    mbar_init(drainb, 1);
     *abort = 0;
+    for (int i = 0; i < 4; ++i) s_issued[i] = 0;
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -318,7 +357,9 @@ __global__ void __launch_bounds__(320, 1)
       c.rank = rank;
       c.abort = abort;
       c.status = a.status;
-      for (int pt = cluster; pt < npair_tiles; pt += nclusters) {
+      c.limit = a.wait_ns;
+      c.issuedA = c.issuedB = 0;
+      for (int pt = cluster; pt < npair_tiles && !a.hold_loads; pt += nclusters) {
         int mp, nt;
         pair_tile_coords(pt, mpairs, a.ntiles, mp, nt);
         const int mt = 2 * mp + (int)rank;
@@ -327,6 +368,14 @@ __global__ void __launch_bounds__(320, 1)
         bool ok = oz2_produce_group<S, kG1>(a, LA, LB, c, rowA0, rowB0);
         if constexpr (NG > 1) ok = ok && oz2_produce_group<S, kG2>(a, LA, LB, c, rowA0, rowB0);
         if (!ok) break;
+      }
+      // The fill counts go to the even CTA, which drains both CTAs' copies.
+      if (rank == 0) {
+        s_issued[0] = c.issuedA;
+        s_issued[1] = c.issuedB;
+      } else {
+        st_cluster_u32(&s_issued[2], 0, c.issuedA);
+        st_cluster_u32(&s_issued[3], 0, c.issuedB);
       }
     }
   } else if (warp == 1) {
@@ -343,12 +392,16 @@ __global__ void __launch_bounds__(320, 1)
       c.emptyB = emptyB;
       c.abort = abort;
       c.status = a.status;
+      c.limit = a.wait_ns;
       for (int pt = cluster; pt < npair_tiles; pt += nclusters) {
         if (!oz2_mma_group<S, kG1>(a, LA, LB, accpar, c, acce, accf)) break;
         if constexpr (NG > 1)
           if (!oz2_mma_group<S, kG2>(a, LA, LB, accpar, c, acce, accf)) break;
       }
+      // Every MMA issued is complete (in both CTAs) before TMEM is released.
+      tc_commit_pair(drainb);
     }
+    if (lane == 0) mbar_wait_drain(drainb, 0, a.status, a.wait_ns);
   } else {
     const int q = warp & 3;
     const int h = (warp - 2) >> 2;
@@ -401,14 +454,12 @@ __global__ void __launch_bounds__(320, 1)
   }
   __syncwarp();
   tc_fence_before();
-  __syncthreads();
-  if (*abort) {
-    // Let MMAs and copies already in flight finish before TMEM goes away.
-    const uint64_t t0 = globaltimer_ns();
-    while (globaltimer_ns() - t0 < 2000000ull) {
-    }
+  cluster_sync();  // both CTAs' fill counts are in; every MMA is complete
+  if (rank == 0 && warp == 0 && lane == 0) {
+    oz2_drain_ring(fullA, kOzRingA, s_issued[0], s_issued[2], 16384u, a.status, a.wait_ns);
+    oz2_drain_ring(fullB, kOzRingB, s_issued[1], s_issued[3], kOzHalfB, a.status, a.wait_ns);
   }
-  cluster_sync();  // no remote arrive or multicast commit is still pending
+  cluster_sync();  // every copy has landed; no remote arrive is still pending
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc_pair(tmem, 512);

@@ -19,6 +19,7 @@ struct OzMmaCtx {
   uint64_t *full, *empty;
   volatile int *abort;
   int *status;
+  uint64_t limit;    // wait bound (ns)
 };
 
 template <int S, int GI, int ST>
@@ -31,8 +32,8 @@ __device__ __forceinline__ bool oz_mma_step(OzMmaCtx &c) {
   uint32_t sla, pa, slb, pb;
   oz_slot(c.s0, c.par0, la, sla, pa);
   oz_slot(c.s0, c.par0, lb, slb, pb);
-  if (wait_a && !mbar_wait(&c.full[sla], pa, c.abort, c.status, QS_ETIMEOUT)) return false;
-  if (wait_b && !mbar_wait(&c.full[slb], pb, c.abort, c.status, QS_ETIMEOUT)) return false;
+  if (wait_a && !mbar_wait(&c.full[sla], pa, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
+  if (wait_b && !mbar_wait(&c.full[slb], pb, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
   if (wait_a || wait_b) tc_fence_after();
   const uint32_t d = c.tmem + acc * 128;
   const uint64_t adesc = sw128_kmajor_desc(c.slots_u32 + sla * TILE);
@@ -65,6 +66,8 @@ struct OzLoadCtx {
   uint64_t *full, *empty;
   volatile int *abort;
   int *status;
+  uint64_t limit;   // wait bound (ns)
+  uint32_t issued;  // fills issued, in ring order (the exit drain's count)
 };
 
 template <int S, int GI, int LD>
@@ -73,10 +76,11 @@ __device__ __forceinline__ bool oz_load(OzLoadCtx &c) {
   constexpr uint32_t TILE = 128 * 128;
   uint32_t slot, par;
   oz_slot(c.s0, c.par0, LD, slot, par);
-  if (!mbar_wait(&c.empty[slot], par ^ 1u, c.abort, c.status, QS_ETIMEOUT)) return false;
+  if (!mbar_wait(&c.empty[slot], par ^ 1u, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
   mbar_arrive_expect_tx(&c.full[slot], TILE);
   const uint8_t *src = side == 0 ? c.rowA + slice * c.planeA : c.rowB + slice * c.planeB;
   bulk_g2s(c.slots + slot * TILE, src, TILE, &c.full[slot]);
+  ++c.issued;
   return true;
 }
 
@@ -113,7 +117,7 @@ __device__ __forceinline__ bool oz_mma_group(const GemmArgs &a, uint32_t &L, uin
   for (int ks = 0; ks < a.nkseg; ++ks) {
 #pragma unroll
     for (int q = 0; q < NACC; ++q)
-      if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, c.abort, c.status, QS_ETIMEOUT)) return false;
+      if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, c.abort, c.status, QS_ETIMEOUT, c.limit)) return false;
     tc_fence_after();
     c.started = 0;
     const int kb0 = ks * a.kseg_blocks, kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
@@ -142,7 +146,7 @@ __device__ __forceinline__ bool oz_drain_group(const GemmArgs &a, uint32_t &accp
   for (int ks = 0; ks < a.nkseg; ++ks) {
 #pragma unroll
     for (int qa = 0; qa < NACC; ++qa) {
-      if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT)) return false;
+      if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT, a.wait_ns)) return false;
       tc_fence_after();
       const double w = a.wdiag[T0 + qa];
 #pragma unroll
@@ -180,7 +184,8 @@ __global__ void __launch_bounds__(320, 1)
   uint8_t *slots = smem;
   uint64_t *bars = (uint64_t *)(slots + kOzSlots * TILE);
   uint64_t *full = bars, *empty = bars + kOzSlots, *accf = bars + 2 * kOzSlots, *acce = accf + 4;
-  uint32_t *tmem_slot = (uint32_t *)(acce + 4);
+  uint64_t *drainb = acce + 4;  // the MMA thread's exit drain
+  uint32_t *tmem_slot = (uint32_t *)(drainb + 1);
   volatile int *abort = (volatile int *)(tmem_slot + 1);
   int64_t *s_offN = (int64_t *)(smem + kOzSlots * TILE + 1024);
   int32_t *s_expN = (int32_t *)(s_offN + 128);
@@ -197,6 +202,7 @@ __global__ void __launch_bounds__(320, 1)
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 8);
     }
+    mbar_init(drainb, 1);
     *abort = 0;
     fence_mbar_init();
   }
@@ -219,7 +225,9 @@ __global__ void __launch_bounds__(320, 1)
       c.empty = empty;
       c.abort = abort;
       c.status = a.status;
-      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+      c.limit = a.wait_ns;
+      c.issued = 0;
+      for (int tile = blockIdx.x; tile < ntile_total && !a.hold_loads; tile += gridDim.x) {
         int lt;
         const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
         int mt, nt;
@@ -232,6 +240,8 @@ __global__ void __launch_bounds__(320, 1)
         if constexpr (NG > 1)
           if (!oz_produce_group<S, kG2>(P, L, c, tileA, tileB)) break;
       }
+      // No copy may still be landing in this CTA's shared memory at exit.
+      drain_ring(full, kOzSlots, c.issued, a.status, a.wait_ns);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -243,6 +253,7 @@ __global__ void __launch_bounds__(320, 1)
       c.empty = empty;
       c.abort = abort;
       c.status = a.status;
+      c.limit = a.wait_ns;
       for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
         int lt;
         const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
@@ -250,6 +261,9 @@ __global__ void __launch_bounds__(320, 1)
         if constexpr (NG > 1)
           if (!oz_mma_group<S, kG2>(P, L, accpar, c, acce, accf)) break;
       }
+      // Every MMA this thread issued is complete before TMEM is released.
+      tc_commit(drainb);
+      mbar_wait_drain(drainb, 0, a.status, a.wait_ns);
     }
   } else {
     const int q = warp & 3;
@@ -314,11 +328,6 @@ __global__ void __launch_bounds__(320, 1)
   __syncwarp();
   tc_fence_before();
   __syncthreads();
-  if (*abort) {
-    const uint64_t t0 = globaltimer_ns();
-    while (globaltimer_ns() - t0 < 2000000ull) {
-    }
-  }
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);

@@ -7,6 +7,8 @@
 
 #include <cstdint>
 
+#include "../../include/qsgpu.h"
+
 namespace qs {
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -48,22 +50,57 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 
 // A wait that gives up: after `limit_ns` of waiting (or once another role
 // raised `abort`), it records `code` in the status word, raises `abort` and
-// returns false.  Every wait in the tensor-core kernels goes through here.
+// returns false.  Every wait of a kernel's roles goes through here; the limit
+// is the plan's (GemmArgs::wait_ns, 2 s unless qs_plan_set_wait_limit).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
-                                          int *status, int code) {
+                                          int *status, int code, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 0;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if ((it & 255u) == 255u && globaltimer_ns() - t0 > kWaitLimitNs) {
+    if ((it & 255u) == 255u && globaltimer_ns() - t0 > limit_ns) {
       *abort = 1;
       if (status) atomicExch(status, code);
       return false;
     }
   }
+}
+
+// The exit drain's wait: the same bound, but it does not give up when
+// `abort` is raised (the drain runs because of it).  False on timeout, with
+// QS_ETIMEOUT in the status word.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t *bar, uint32_t parity, int *status, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 255u && globaltimer_ns() - t0 > limit_ns) {
+      if (status) atomicExch(status, QS_ETIMEOUT);
+      return false;
+    }
+  }
+}
+
+// Before a CTA exits: wait for every bulk copy this thread issued into a
+// ring of `nslots` full barriers, `issued` fills in ring order (fill i went
+// to slot i % nslots in phase i / nslots).  A slot's fills complete in order,
+// so waiting for its last fill covers the earlier ones.  Instant when every
+// fill was consumed; bounded when a wait gave up with copies still landing.
+__device__ __forceinline__ void drain_ring(uint64_t *full, int nslots, uint32_t issued, int *status,
+                                           uint64_t limit_ns) {
+  for (int s = 0; s < nslots; ++s) {
+    if (issued <= (uint32_t)s) break;
+    const uint32_t last = (issued - 1u - (uint32_t)s) / (uint32_t)nslots;
+    mbar_wait_drain(&full[s], last & 1u, status, limit_ns);
+  }
+}
+
+// Count `bytes` of the current phase's transaction as done without a copy.
+__device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
 // --------------------------------------------------------- bulk copies ---
@@ -179,6 +216,10 @@ __device__ __forceinline__ uint32_t mapa_u32(const void *p, uint32_t cta) {
   uint32_t r;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(cta));
   return r;
+}
+// Store a word at `p`'s offset in CTA `cta`'s shared memory.
+__device__ __forceinline__ void st_cluster_u32(const void *p, uint32_t cta, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(mapa_u32(p, cta)), "r"(v) : "memory");
 }
 // Tiled 2-D tensor load (no multicast) into this CTA's shared memory whose
 // byte count completes on the mbarrier at shared::cluster address `mbar`,

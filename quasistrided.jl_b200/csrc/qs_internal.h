@@ -7,9 +7,20 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/qsgpu.h"
 
 namespace qs {
+
+// An NVTX range over a scope (plan, execute, group execute): visible in
+// Nsight timelines, a no-op unless a profiler is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 constexpr int kMaxRank = 16;  // labels per M/N/K composite
 
@@ -118,6 +129,10 @@ struct qs_plan {
   std::string bounds_msg;
   int host_only = 0;
   int device = 0;
+  // Tensor-core kernels: bound of every barrier wait, and the failure-
+  // detection hold (qs_plan_set_wait_limit).
+  uint64_t wait_ns = 2000000000ull;
+  int hold_loads = 0;
   qs_plan_options opts{};
   // Workspace allocator (qs_plan_options.allocator), copied; has_alloc == 0
   // means the library's stream-ordered pool.  last_stream is the stream of

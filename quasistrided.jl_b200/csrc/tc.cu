@@ -396,6 +396,9 @@ struct GemmArgs {
              // row i; 2 = planar: real columns 2n / 2n+1 are Re / Im of n
   int *status;
   double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
+  uint64_t wait_ns;  // bound of every barrier wait (qs_plan_set_wait_limit)
+  int hold_loads;    // failure-detection test: the producers issue no copies
+  int pad_;
 };
 
 // The alpha/beta store of one 16-column chunk of a row of the tile, values
@@ -662,7 +665,8 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   uint8_t *sB = smem + STAGES * A_BYTES;
   uint64_t *bars = (uint64_t *)(sB + STAGES * B_BYTES);
   uint64_t *full = bars, *empty = bars + STAGES, *accf = bars + 2 * STAGES, *acce = accf + 2;
-  uint32_t *tmem_slot = (uint32_t *)(acce + 2);
+  uint64_t *drainb = acce + 2;  // the MMA thread's exit drain
+  uint32_t *tmem_slot = (uint32_t *)(drainb + 1);
   volatile int *abort = (volatile int *)(tmem_slot + 1);
   int64_t *s_offN = (int64_t *)(smem + STAGES * (A_BYTES + B_BYTES) + 1024);
   int32_t *s_expN = (int32_t *)(s_offN + BN);
@@ -677,6 +681,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 4);
     }
+    mbar_init(drainb, 1);
     *abort = 0;
     fence_mbar_init();
   }
@@ -689,12 +694,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int ntile_total = gt.nprob ? gt.tile_start[gt.nprob] : a.mtiles * a.ntiles;
+  uint32_t issued = 0;  // the producer's fills, in ring order (the exit drain's count)
 
   if (warp == 0) {
     // ---------------------------------------------------- producer ----
     if (lane == 0) {
       uint32_t stage = 0, phase = 0;
-      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+      for (int tile = blockIdx.x; tile < ntile_total && !a.hold_loads; tile += gridDim.x) {
         int lt;
         const GemmArgs &P = gt.nprob ? tile_problem<true>(a, gt, tile, lt) : tile_problem<false>(a, gt, tile, lt);
         const int mt = lt / P.ntiles, nt = lt % P.ntiles;
@@ -709,10 +715,11 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             const uint8_t *srcA = P.panelA + pa * P.planeA + ((int64_t)mt * P.kblocks) * A_BYTES;
             const uint8_t *srcB = P.panelB + pb * P.planeB + ((int64_t)nt * P.kblocks) * B_BYTES;
             for (int kb = kb0; kb < kb1; ++kb) {
-              if (!mbar_wait(&empty[stage], phase ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+              if (!mbar_wait(&empty[stage], phase ^ 1, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
               mbar_arrive_expect_tx(&full[stage], A_BYTES + B_BYTES);
               bulk_g2s(sA + stage * A_BYTES, srcA + (int64_t)kb * A_BYTES, A_BYTES, &full[stage]);
               bulk_g2s(sB + stage * B_BYTES, srcB + (int64_t)kb * B_BYTES, B_BYTES, &full[stage]);
+              ++issued;
               if (++stage == STAGES) {
                 stage = 0;
                 phase ^= 1;
@@ -732,7 +739,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const int nseg = seg_count(P, KIND);
         for (int g = 0; g < nseg; ++g, ++sc) {
           const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
-          if (!mbar_wait(&acce[buf], ap ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+          if (!mbar_wait(&acce[buf], ap ^ 1, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
           tc_fence_after();
           const uint32_t d = tmem + buf * BN;
           int kb0, kb1;
@@ -741,7 +748,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
           uint32_t acc = 0;
           for (int j = 0; j < nt_terms; ++j) {
             for (int kb = kb0; kb < kb1; ++kb) {
-              if (!mbar_wait(&full[stage], phase, abort, a.status, QS_ETIMEOUT)) goto done;
+              if (!mbar_wait(&full[stage], phase, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
               tc_fence_after();
               const uint32_t a0 = smem_u32(sA + stage * A_BYTES), b0 = smem_u32(sB + stage * B_BYTES);
 #pragma unroll
@@ -789,7 +796,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
       const bool row_store = row_ok && eA != kNonFinite;
       for (int g = 0; g < nseg; ++g, ++sc) {
         const uint32_t buf = sc & 1, ap = (sc >> 1) & 1;
-        if (!mbar_wait(&accf[buf], ap, abort, P.status, QS_ETIMEOUT)) goto done;
+        if (!mbar_wait(&accf[buf], ap, abort, P.status, QS_ETIMEOUT, a.wait_ns)) goto done;
         tc_fence_after();
         const bool first = (g == 0), last = (g == nseg - 1);
         const uint32_t tacc = tmem + lane_base + buf * BN;
@@ -838,15 +845,16 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     }
   }
 done:
+  // Before TMEM is released and the CTA exits: every copy the producer issued
+  // has landed and every MMA is complete (instant after a normal run).
+  if (warp == 0 && lane == 0) drain_ring(full, STAGES, issued, a.status, a.wait_ns);
+  if (warp == 1 && lane == 0) {
+    tc_commit(drainb);
+    mbar_wait_drain(drainb, 0, a.status, a.wait_ns);
+  }
   __syncwarp();
   tc_fence_before();
   __syncthreads();
-  if (*abort) {
-    // Give in-flight copies and MMAs time to land before TMEM is released.
-    const uint64_t t0 = globaltimer_ns();
-    while (globaltimer_ns() - t0 < 2000000ull) {
-    }
-  }
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
@@ -898,7 +906,8 @@ __global__ void __launch_bounds__(320, 1)
   uint8_t *slots = smem;
   uint64_t *bars = (uint64_t *)(slots + kOzSlots * TILE);
   uint64_t *full = bars, *empty = bars + kOzSlots, *accf = bars + 2 * kOzSlots, *acce = accf + 4;
-  uint32_t *tmem_slot = (uint32_t *)(acce + 4);
+  uint64_t *drainb = acce + 4;  // the MMA thread's exit drain
+  uint32_t *tmem_slot = (uint32_t *)(drainb + 1);
   volatile int *abort = (volatile int *)(tmem_slot + 1);
   int64_t *s_offN = (int64_t *)(smem + kOzSlots * TILE + 1024);
   int32_t *s_expN = (int32_t *)(s_offN + 128);
@@ -921,6 +930,7 @@ __global__ void __launch_bounds__(320, 1)
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 8);
     }
+    mbar_init(drainb, 1);
     *abort = 0;
     fence_mbar_init();
     for (int gi = 0; gi < sch.ngroups; ++gi) {
@@ -944,12 +954,13 @@ __global__ void __launch_bounds__(320, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int ntile_total = a.mtiles * a.ntiles;
+  uint32_t issued = 0;  // the producer's fills, in ring order (the exit drain's count)
 
   if (warp == 0) {
     // ---------------------------------------------------- producer ----
     if (lane == 0) {
       uint32_t L = 0;
-      for (int tile = blockIdx.x; tile < ntile_total; tile += gridDim.x) {
+      for (int tile = blockIdx.x; tile < ntile_total && !a.hold_loads; tile += gridDim.x) {
         const int mt = tile / a.ntiles, nt = tile % a.ntiles;
         for (int gi = 0; gi < sch.ngroups; ++gi) {
           const GMeta G = s_meta[gi];
@@ -958,7 +969,7 @@ __global__ void __launch_bounds__(320, 1)
             for (int kb = kb0; kb < kb1; ++kb) {
               for (int l = 0; l < G.nloads; ++l, ++L) {
                 const uint32_t slot = L % kOzSlots, round = L / kOzSlots;
-                if (!mbar_wait(&empty[slot], (round & 1) ^ 1, abort, a.status, QS_ETIMEOUT)) goto done;
+                if (!mbar_wait(&empty[slot], (round & 1) ^ 1, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
                 mbar_arrive_expect_tx(&full[slot], TILE);
                 const int code = s_load[gi * kOzMaxLoads + l];
                 const uint8_t *src =
@@ -966,6 +977,7 @@ __global__ void __launch_bounds__(320, 1)
                         ? a.panelA + (code & 15) * a.planeA + ((int64_t)mt * a.kblocks + kb) * TILE
                         : a.panelB + (code & 15) * a.planeB + ((int64_t)nt * a.kblocks + kb) * TILE;
                 bulk_g2s(slots + slot * TILE, src, TILE, &full[slot]);
+                ++issued;
               }
             }
           }
@@ -983,7 +995,7 @@ __global__ void __launch_bounds__(320, 1)
           const int nacc = G.t1 - G.t0 + 1;
           for (int ks = 0; ks < a.nkseg; ++ks) {
             for (int q = 0; q < nacc; ++q)
-              if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, abort, a.status, QS_ETIMEOUT)) goto done;
+              if (!mbar_wait(&acce[q], ((accpar >> q) & 1u) ^ 1u, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
             tc_fence_after();
             uint32_t started = 0;
             const int kb0 = ks * a.kseg_blocks, kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
@@ -998,7 +1010,8 @@ __global__ void __launch_bounds__(320, 1)
                   const int l = u ? lb : la;
                   if (!((waited >> l) & 1u)) {
                     const uint32_t gl = base + l;
-                    if (!mbar_wait(&full[gl % kOzSlots], (gl / kOzSlots) & 1, abort, a.status, QS_ETIMEOUT))
+                    if (!mbar_wait(&full[gl % kOzSlots], (gl / kOzSlots) & 1, abort, a.status, QS_ETIMEOUT,
+                                   a.wait_ns))
                       goto done;
                     waited |= 1u << l;
                   }
@@ -1060,7 +1073,7 @@ __global__ void __launch_bounds__(320, 1)
         const int nacc = G.t1 - G.t0 + 1;
         for (int ks = 0; ks < a.nkseg; ++ks) {
           for (int qa = 0; qa < nacc; ++qa) {
-            if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT)) goto done;
+            if (!mbar_wait(&accf[qa], (accpar >> qa) & 1u, abort, a.status, QS_ETIMEOUT, a.wait_ns)) goto done;
             tc_fence_after();
             const double w = a.wdiag[G.t0 + qa];
             const uint32_t taddr = tmem + lane_base + qa * 128 + 64 * h;
@@ -1091,14 +1104,16 @@ __global__ void __launch_bounds__(320, 1)
     }
   }
 done:
+  // Before TMEM is released and the CTA exits: every copy the producer issued
+  // has landed and every MMA is complete (instant after a normal run).
+  if (warp == 0 && lane == 0) drain_ring(full, kOzSlots, issued, a.status, a.wait_ns);
+  if (warp == 1 && lane == 0) {
+    tc_commit(drainb);
+    mbar_wait_drain(drainb, 0, a.status, a.wait_ns);
+  }
   __syncwarp();
   tc_fence_before();
   __syncthreads();
-  if (*abort) {
-    const uint64_t t0 = globaltimer_ns();
-    while (globaltimer_ns() - t0 < 2000000ull) {
-    }
-  }
   if (warp == 1) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
@@ -1578,6 +1593,9 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.beta_case = beta_case;
   a.status = p->ws.status;
   for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
+  a.wait_ns = p->wait_ns;
+  a.hold_loads = p->hold_loads;
+  a.pad_ = 0;
   return a;
 }
 

@@ -238,3 +238,16 @@ def test_host_only_plan_cannot_execute(qs):
     with pytest.raises(qs.ArgumentError):
         # CPU operands are refused for a device plan: there is no CPU fallback
         qs.plan_contract(C, A, (1, 2), B, (2, 3), (1, 3))
+
+
+def test_wait_limit_validation_on_host(qs):
+    # qs_plan_set_wait_limit: 0 restores the default, limits above 60 s are
+    # not bounds (ArgumentError); a host-only plan accepts the setting.
+    C = qs.StridedView(torch.zeros(6, dtype=torch.float64), (2, 3), (1, 2))
+    A = qs.StridedView(torch.zeros(8, dtype=torch.float64), (2, 4), (1, 2))
+    B = qs.StridedView(torch.zeros(12, dtype=torch.float64), (4, 3), (1, 4))
+    plan = qs.plan_contract(C, A, (1, 2), B, (2, 3), (1, 3), host_only=True)
+    qs.set_wait_limit(plan, 1_000_000, hold_loads=True)
+    qs.set_wait_limit(plan, 0)
+    with pytest.raises(qs.ArgumentError, match="60 s"):
+        qs.set_wait_limit(plan, 61_000_000_000)
