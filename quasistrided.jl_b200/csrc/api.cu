@@ -429,7 +429,7 @@ int qs_plan_contract(qs_plan **out, const qs_view *C, const qs_view *A, const in
   const int nt = p->opts.native_tile;
   if (nt < 0 || nt > kNativeShapes) {
     delete p;
-    return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..9");
+    return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..10");
   }
   p->native_shape = native_shape_for(p->T, p->TA, p->TB, p->M, p->N, p->K, nt, false);
   if (!p->host_only) {

@@ -284,6 +284,8 @@ template <>
 struct DmmaShape<3> { using Cfg = DmmaCfg<128, 32, 8, 1, 4>; };
 template <>
 struct DmmaShape<4> { using Cfg = DmmaCfg<256, 16, 8, 1, 4>; };
+template <>
+struct DmmaShape<5> { using Cfg = DmmaCfg<128, 128, 4, 4, 4>; };
 
 void dmma_tile_dims(int shape, int *bm, int *bn) {
   switch (shape) {
@@ -291,6 +293,7 @@ void dmma_tile_dims(int shape, int *bm, int *bn) {
     case 2: *bm = 64; *bn = 64; break;
     case 3: *bm = 128; *bn = 32; break;
     case 4: *bm = 256; *bn = 16; break;
+    case 5: *bm = 128; *bn = 128; break;
     default: *bm = 128; *bn = 128; break;
   }
 }
@@ -346,6 +349,7 @@ cudaError_t launch_dmma(const Operands &op, const double *alpha, const double *b
     case 2: return launch_dmma_s<2>(op, s, a_mfast, b_nfast, st);
     case 3: return launch_dmma_s<3>(op, s, a_mfast, b_nfast, st);
     case 4: return launch_dmma_s<4>(op, s, a_mfast, b_nfast, st);
+    case 5: return launch_dmma_s<5>(op, s, a_mfast, b_nfast, st);
     default: return launch_dmma_s<0>(op, s, a_mfast, b_nfast, st);
   }
 }
@@ -366,6 +370,7 @@ cudaError_t dmma_group_launch(int shape, const void *jobs, int njobs, int blocks
     case 2: return dmma_group_launch_s<2>(jobs, njobs, blocks, st);
     case 3: return dmma_group_launch_s<3>(jobs, njobs, blocks, st);
     case 4: return dmma_group_launch_s<4>(jobs, njobs, blocks, st);
+    case 5: return dmma_group_launch_s<5>(jobs, njobs, blocks, st);
     default: return dmma_group_launch_s<0>(jobs, njobs, blocks, st);
   }
 }

@@ -50,8 +50,9 @@ int direct_shape_mn(int T, int64_t M, int64_t N);
 // Native-method tile shapes, as stored in a plan (qs_plan_info.native_tile
 // is the shape + 1): 0-3 the SIMT gather GEMM's tiles (direct_shape
 // numbering), 4 + s the DMMA kernel's tile s (0: 128x128, 1: 128x64,
-// 2: 64x64, 3: 128x32, 4: 256x16), for real Float64 operands only.
-constexpr int kSimtShapes = 4, kDmmaShapes = 5, kNativeShapes = kSimtShapes + kDmmaShapes;
+// 2: 64x64, 3: 128x32, 4: 256x16, 5: 128x128 with 16 warps), for real
+// Float64 operands only.
+constexpr int kSimtShapes = 4, kDmmaShapes = 6, kNativeShapes = kSimtShapes + kDmmaShapes;
 // The shape for compute type T with operand eltypes TA, TB: native_tile
 // (1..kNativeShapes) if it applies, else by M and N (grouped: by N only,
 // since the group's other problems fill the GPU).  Skinny problems (the

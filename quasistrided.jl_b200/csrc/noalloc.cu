@@ -124,7 +124,7 @@ extern "C" int qs_contract_noalloc(const qs_view *C, const double *alpha, const 
     return fail(QS_EINVAL, s.str());
   }
   const int nt = o.native_tile;
-  if (nt < 0 || nt > kNativeShapes) return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..9");
+  if (nt < 0 || nt > kNativeShapes) return fail(QS_EINVAL, "ArgumentError: native_tile must be 0..10");
   const int acase = scalar_case(p.T, alpha), bcase = scalar_case(p.T, beta);
   const bool scale_only = acase == 0 || p.path == QS_PATH_SCALE;
   if ((rc = check_bounds(&p, !scale_only))) return rc;
