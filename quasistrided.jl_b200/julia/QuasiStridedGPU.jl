@@ -191,6 +191,28 @@ function execute!(p::ContractPlan, alpha::Number, beta::Number)
 end
 
 """
+    check_status(p::ContractPlan)
+
+Synchronizes CUDA.jl's stream and throws if a bounded device wait of the
+plan's tensor-core kernels gave up since the last check (QS_ETIMEOUT): the
+kernel stopped without writing C; the plan stays usable.
+"""
+check_status(p::ContractPlan) =
+    check(ccall((:qs_plan_check_status, libqsgpu), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), p.handle,
+        reinterpret(Ptr{Cvoid}, CUDA.stream().handle)))
+
+"""
+    set_wait_limit!(p::ContractPlan, limit_ns = 0; hold_loads = false)
+
+Bound every device wait of the plan's tensor-core kernels (0: the default
+2 s); `hold_loads` makes a wait run out with nothing in flight, for tests of
+the failure path.
+"""
+set_wait_limit!(p::ContractPlan, limit_ns::Integer = 0; hold_loads::Bool = false) =
+    check(ccall((:qs_plan_set_wait_limit, libqsgpu), Cint, (Ptr{Cvoid}, UInt64, Int32), p.handle,
+        UInt64(limit_ns), Int32(hold_loads)))
+
+"""
     contract!(C, alpha, A, indA, B, indB, beta, indC; accumulator = nothing) -> C
 """
 function contract!(C::DeviceStridedView, alpha::Number, A::DeviceStridedView, indA, B::DeviceStridedView,
