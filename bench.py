@@ -177,6 +177,16 @@ STAGE_NAMES = {"ozaki": ["pack", "pack_none", "gemm_i8", "fixup"],
                "native": ["gemm_native"]}
 
 
+def library_peaks():
+    """cuBLAS INT8 and FP64 GEMM throughput measured on this pool by
+    `bench.py --peaks` (profiles/library_peaks_b200.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "library_peaks_b200.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
 def load_ncu_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -190,10 +200,12 @@ def load_ncu_traffic(kernel):
 def roofline(plan, stage_ms, nexec):
     """Roofline of the dominant kernel from the per-stage CUDA-event times of
     the timed region.  Ozaki GEMM: algorithmic work = the slice products,
-    s(s+1)/2 * 2MNK int8 ops; peak = 2x the measured dense bf16 figure (the
-    B200's int8:bf16 dense ratio; no int8 figure is measured by the driver).
-    Native GEMM: 2MNK fp64 flops against the B200's nominal 40 TFLOP/s FP64."""
+    s(s+1)/2 * 2MNK int8 ops; peak = the measured cuBLAS int8 GEMM of
+    profiles/library_peaks_b200.json (else 2x the dense bf16 figure).  Native
+    GEMM: 2MNK fp64 flops against the measured cuBLAS DGEMM (else the
+    nominal 40 TFLOP/s)."""
     peaks, kind = measured_peaks()
+    lib = library_peaks()
     names = STAGE_NAMES.get(plan.method, [f"stage{i}" for i in range(len(stage_ms))])
     per = {names[i] if i < len(names) else f"stage{i}": stage_ms[i] / max(nexec, 1)
            for i in range(len(stage_ms))}
@@ -201,8 +213,12 @@ def roofline(plan, stage_ms, nexec):
         s = plan.ozaki_slices
         work = s * (s + 1) / 2 * FLOPS
         ms = per.get("gemm_i8")
-        peak = 2.0 * peaks["bf16_tflops"]
-        note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
+        if lib:
+            peak = lib["int8_int_mm_tops"]
+            note = "measured cuBLAS int8 GEMM (torch._int_mm 8192^3) on this pool"
+        else:
+            peak = 2.0 * peaks["bf16_tflops"]
+            note = f"int8 dense peak = 2 x {kind} bf16 dense ({peaks['bf16_tflops']} TFLOP/s)"
         if s in (4, 6, 7) and not plan.per_product_gemm:
             kernel = f"oz_gemm_fixed_kernel<{s}, false>" if plan.oz_single_sm else f"oz_gemm_pair_kernel<{s}>"
         else:
@@ -216,9 +232,13 @@ def roofline(plan, stage_ms, nexec):
     else:
         work = FLOPS
         ms = per.get("gemm_native")
-        peak = 40.0
-        note = "nominal B200 FP64 (no measured FP64 figure)"
-        kernel = "direct_gemm_kernel"
+        if lib:
+            peak = lib["fp64_cublas_tflops"]
+            note = "measured cuBLAS DGEMM (8192^3) on this pool"
+        else:
+            peak = 40.0
+            note = "nominal B200 FP64"
+        kernel = "dmma_gemm_kernel" if getattr(plan, "native_tile", 0) >= 5 else "direct_gemm_kernel"
     achieved = work / (ms * 1e-3) / 1e12 if ms else None
     roof = {"bound": "tensor", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None, "traffic": load_ncu_traffic(kernel),
