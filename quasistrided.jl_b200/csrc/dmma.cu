@@ -25,6 +25,7 @@
 // Zero/One/beta cases and one rounding to eltype(C), as in the gather GEMM.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <cstring>
@@ -318,9 +319,20 @@ int dmma_shape_mn(int64_t M, int64_t N) {
   return s;
 }
 
+// The dynamic shared-memory opt-in of one kernel instance, set on the
+// first launch on each device (a per-launch driver call costs microseconds
+// on the one-shot contract path).
 template <class Cfg, class K>
 static cudaError_t dmma_smem_attr(K kernel) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 63;
+  const uint64_t bit = 1ull << dev;
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+  return e;
 }
 
 template <int SHAPE>
