@@ -165,7 +165,8 @@ typedef struct qs_plan_options {
                               1 = 64x64, 2 = 128x32, 3 = 256x16, 4 = 32x32 (real
                               compute types); DMMA kernel (real Float64 A and B)
                               5 = 128x128, 6 = 128x64, 7 = 64x64, 8 = 128x32,
-                              9 = 256x16 (the autotuner's knob) */
+                              9 = 256x16, 10 = 128x128 with 16 warps (the
+                              autotuner's knob) */
   const qs_allocator *allocator; /* plan workspace from here; NULL = the library's
                                     stream-ordered pool (DefaultAllocator) */
 } qs_plan_options;
@@ -186,7 +187,7 @@ typedef struct qs_plan_info {
   int64_t workspace_bytes;
   int32_t stride_class;  /* bit 0: A's M map unit-stride, bit 1: B's N map,
                             bit 2: C's M map (the autotuner's stride class) */
-  int32_t native_tile;   /* native-method tile in use (1..9 as in the options) */
+  int32_t native_tile;   /* native-method tile in use (1..10 as in the options) */
   int32_t batch_rank;    /* batch labels (QS_PLAN_BATCH_LABELS), 0 without */
   int64_t batch_length;  /* product of their extents (1 without) */
   int64_t batch_labels[16];

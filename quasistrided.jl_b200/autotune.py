@@ -96,12 +96,12 @@ class Autotuner:
     def candidates(hp, dmma: bool = False) -> list:
         """Options to time for a problem class; `dmma`: A and B are real
         Float64 in a Float64 computation, so the DMMA kernel's tiles
-        (native_tile 5..9) are candidates beside the SIMT tiles (1..4)."""
+        (native_tile 5..10) are candidates beside the SIMT tiles (1..4)."""
         real = not hp.compute_type.startswith("Complex")
         dbl = hp.compute_type in ("Float64", "ComplexF64")
         out = []
         if real:
-            tiles = (1, 2, 3, 4, 5, 6, 7, 8, 9) if dmma else (1, 2, 3, 4)
+            tiles = tuple(range(1, 11)) if dmma else (1, 2, 3, 4)
             out += [{"method": "native", "native_tile": t} for t in tiles]
         else:
             out.append({"method": "native"})

@@ -103,6 +103,19 @@ __device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes) 
   asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// ------------------------------------------------------------ cp.async ---
+// Per-thread asynchronous global -> shared copies of 4, 8 or 16 bytes
+// (src-size 0 zero-fills), grouped with commit/wait.
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // --------------------------------------------------------- bulk copies ---
 // Non-tensor bulk copy global -> this CTA's shared memory, completing on an
 // mbarrier transaction count.  Both addresses 16-byte aligned, size a

@@ -216,160 +216,248 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 }
 
 // Fused Ozaki pack: both passes in one launch, each operand read once from
-// HBM.  A CTA walks bands of kBandRows rows of one operand (A's bands, then
-// B's).  Phase 1 streams the band's K tiles and reduces every row's max
-// |x| bit pattern in registers (no atomics, nothing to clear per execute);
-// phase 2 streams the band again and emits the digit planes.  The grid is a
-// few CTAs per SM, so the bands in flight (kBandRows * K * 8 bytes each)
-// stay in L2 between the two phases and phase 2 reads them from there.
-constexpr int kBandRows = 8, kBandK = 512;
-constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 double per 16, +4 per row: conflict-free
+// HBM.  A CTA walks bands of kBandRows (virtual) rows of one operand.
+// Phase 1 streams the band's K tiles and reduces every row's max |x| bit
+// pattern in registers (no atomics, nothing to clear per execute); phase 2
+// streams the band again and emits the digit planes.  The grid is two CTAs
+// per SM, so the bands in flight (kBandRows * K * 8 bytes each) stay in L2
+// between the two phases and phase 2 reads them from there.
+//
+// The tiles move by cp.async into a kPackBufs-deep ring, kPackBufs - 1
+// tiles ahead of the one being processed and across band boundaries, so
+// every CTA keeps a tile of loads in flight (a pack with synchronous loads
+// left HBM at 8 % of its bandwidth).  The copies are raw element bytes: a
+// tile slot holds one real value or one complex component (Float32 in its
+// low four bytes), and the virtual matrix (type conversion, conj, the 1e /
+// 1r complex layouts) is formed when a slot is read.
+constexpr int kBandRows = 8, kBandK = 512, kPackBufs = 3;
+constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 slot per 16, +4 per row: conflict-free
+constexpr size_t kPackSmem = (size_t)kPackBufs * kBandRows * kBandStride * 8;
 
 __device__ __forceinline__ int band_col(int k) { return k + (k >> 4); }
 
-// K tile [k0, k0 + kBandK) of rows [r0, r0 + kBandRows) into `tile`
-// (virtual matrix values, zero outside rows/K), coalesced along X's
-// unit-stride axis.  STREAM: the band's second read (L2, evict first).
-template <bool STREAM>
-__device__ __forceinline__ void load_band(const PackArgs &a, int64_t r0, int64_t k0,
-                                          double (*tile)[kBandStride]) {
+__device__ __forceinline__ void cp_async_4_8(uint32_t saddr, const void *g, int size, bool ok) {
+  if (size == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 8 : 0)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 4 : 0)
+                 : "memory");
+}
+
+// Issue the copies of K tile [k0, k0 + kBandK) of virtual rows
+// [r0, r0 + kBandRows) into `tile` (slot (row, k) at row * kBandStride +
+// band_col(k)), zero-filled outside the operand.  Real operands (cmode 0):
+// slot = element.  1r (cmode 2, K doubled): slots 2j, 2j+1 = re, im of
+// complex K index j.  1e (cmode 1, rows and K doubled): complex row i goes
+// to even row 2i as in 1r; odd rows are formed from it on read.  A real
+// operand in a complex layout gets zero imaginary slots.
+__device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_t k0, uint32_t tile) {
   const int tid = threadIdx.x;
+  const bool cx = a.TX == QS_C32 || a.TX == QS_C64;
+  const int esz = (a.TX == QS_F64 || a.TX == QS_C64) ? 8 : 4;
+  const char *X = static_cast<const char *>(a.X);
+  auto slot = [&](int rr, int kk) {
+    const int64_t r = r0 + rr, k = k0 + kk;
+    const uint32_t dst = tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk));
+    if (a.cmode == 1 && (rr & 1)) return;  // derived from the even row
+    bool ok = r < a.rows && k < a.K;
+    int64_t rix = a.cmode == 1 ? (r >> 1) : r, kix = a.cmode ? (k >> 1) : k;
+    int part = a.cmode ? (int)(k & 1) : 0;
+    if (part && !cx) ok = false;  // imaginary part of a real operand
+    const char *src = X;
+    if (ok) {
+      const int64_t e = a.Xbase + __ldg(a.offR + rix) + __ldg(a.offK + kix);
+      src = X + (cx ? (2 * e + part) : e) * esz;
+    }
+    cp_async_4_8(dst, src, esz, ok);
+  };
   constexpr int PER = kBandRows * kBandK / 256;
-  if (a.cmode == 0 && (a.TX == QS_F64 || a.TX == QS_F32)) {
-    const bool f64 = a.TX == QS_F64;
-    auto ld = [&](int64_t idx) -> double {
-      if (f64) {
-        const double *p = static_cast<const double *>(a.X) + idx;
-        return STREAM ? __ldcs(p) : __ldg(p);
+  if (a.rfast) {
+#pragma unroll 4
+    for (int i = 0; i < PER; ++i) slot(tid % kBandRows, tid / kBandRows + (256 / kBandRows) * i);
+  } else {
+#pragma unroll 4
+    for (int i = 0; i < PER; ++i) slot(i % kBandRows, tid + 256 * (i / kBandRows));
+  }
+}
+
+// Virtual value (row w, K index kk) of a staged tile; k0 + kk >= K reads 0.
+__device__ __forceinline__ double band_raw(const PackArgs &a, const double *tile, int row, int kk) {
+  const double *p = tile + row * kBandStride + band_col(kk);
+  if (a.TX == QS_F64 || a.TX == QS_C64) return *p;
+  return (double)*reinterpret_cast<const float *>(p);
+}
+__device__ __forceinline__ double band_value(const PackArgs &a, const double *tile, int w, int kk) {
+  if (a.cmode == 0) return band_raw(a, tile, w, kk);
+  if (a.cmode == 2) {
+    const double v = band_raw(a, tile, w, kk);
+    return ((kk & 1) && a.conj) ? -v : v;
+  }
+  const int base = w & ~1;
+  const double re = band_raw(a, tile, base, kk & ~1);
+  double im = band_raw(a, tile, base, kk | 1);
+  if (a.conj) im = -im;
+  const int rp = w & 1, kp = kk & 1;
+  return rp == kp ? re : (rp ? im : -im);
+}
+
+// One row band's state for the processing side.
+struct BandState {
+  unsigned long long mb;  // running max |x| bit pattern of this warp's row
+  int E;
+  bool bad;
+};
+
+// Process tile `t` (phase 1: t < nk1; phase 2 otherwise) of the band at
+// r0: warp w owns virtual row r0 + w, lane l its K values 16 l .. 16 l + 15.
+__device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int t, int nk1, const double *tile,
+                                             BandState &bs) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t grow = r0 + w;
+  if (t < nk1) {
+    const int64_t k0 = (int64_t)t * kBandK;
+    if (t == 0) bs.mb = 0;
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      const int k = lane * 16 + kk;
+      const double v = k0 + k < a.K ? band_value(a, tile, w, k) : 0.0;
+      const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
+      bs.mb = b > bs.mb ? b : bs.mb;
+    }
+    if (t == nk1 - 1) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, bs.mb, o);
+        bs.mb = x > bs.mb ? x : bs.mb;
       }
-      const float *p = static_cast<const float *>(a.X) + idx;
-      return (double)(STREAM ? __ldcs(p) : __ldg(p));
-    };
-    if (a.rfast) {
-      const int rr = tid % kBandRows, kb = tid / kBandRows;
-      const int64_t r = r0 + rr;
-      const bool rok = r < a.rows;
-      const int64_t ro = rok ? a.Xbase + __ldg(a.offR + r) : 0;
-#pragma unroll
-      for (int i = 0; i < PER; ++i) {
-        const int kk = kb + (256 / kBandRows) * i;
-        const int64_t k = k0 + kk;
-        const bool ok = rok && k < a.K;
-        tile[rr][band_col(kk)] = ok ? ld(ro + __ldg(a.offK + k)) : 0.0;
+      // E: the row max's frexp exponent + 1; non-finite rows get kNonFinite,
+      // zero digits and a place on the fixup list.
+      bs.E = 0;
+      bs.bad = bs.mb >= 0x7FF0000000000000ull;
+      if (bs.bad) {
+        bs.E = kNonFinite;
+      } else if (bs.mb) {
+        frexp(__longlong_as_double((long long)bs.mb), &bs.E);
+        bs.E += 1;
       }
-    } else {
-#pragma unroll
-      for (int h = 0; h < kBandK / 256; ++h) {
-        const int kk = tid + 256 * h;
-        const int64_t k = k0 + kk;
-        const bool kok = k < a.K;
-        const int64_t ko = kok ? a.Xbase + __ldg(a.offK + k) : 0;
-#pragma unroll
-        for (int rr = 0; rr < kBandRows; ++rr) {
-          const int64_t r = r0 + rr;
-          const bool ok = kok && r < a.rows;
-          tile[rr][band_col(kk)] = ok ? ld(ko + __ldg(a.offR + r)) : 0.0;
-        }
+      if (grow < a.rows_pad && lane == 0) {
+        a.exp_out[grow] = bs.E;
+        if (bs.bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
       }
     }
     return;
   }
-#pragma unroll 4
-  for (int i = 0; i < PER; ++i) {
-    int rr, kk;
-    if (a.rfast) {
-      rr = tid % kBandRows;
-      kk = tid / kBandRows + (256 / kBandRows) * i;
-    } else {
-      kk = tid + 256 * (i % (kBandK / 256));
-      rr = i / (kBandK / 256);
+  const int64_t k0 = (int64_t)(t - nk1) * kBandK;
+  const int64_t kpad = (int64_t)a.kblocks * kKBytes;  // digits per row (bytes = K values)
+  const int64_t kc = k0 + lane * 16;
+  if (grow >= a.rows_pad || kc >= kpad) return;
+  double x[16];
+#pragma unroll
+  for (int kk = 0; kk < 16; ++kk) {
+    const int k = lane * 16 + kk;
+    const double v = k0 + k < a.K ? band_value(a, tile, w, k) : 0.0;
+    x[kk] = (bs.bad || !bs.mb) ? 0.0 : scale2(v, -bs.E);
+  }
+  const int64_t off = panel_tile_base(a, grow, kc);
+  for (int p = 0; p < a.nslices; ++p) {
+    uint32_t wd[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      // y = 254 x; d = y rounded to the nearest integer (ties to even, like
+      // rint) by adding and removing 1.5 * 2^52, whose low word then holds
+      // d in two's complement; x = y - d.  Four full-rate FP64 adds and
+      // multiplies, no rounding or conversion instructions; the _rn
+      // intrinsics keep the compiler from fusing the steps.
+      constexpr double kRound = 6755399441055744.0;
+      const double y = __dmul_rn(x[kk], 254.0);
+      const double tt = __dadd_rn(y, kRound);
+      const double d = __dsub_rn(tt, kRound);
+      x[kk] = __dsub_rn(y, d);
+      wd[kk >> 2] |= ((uint32_t)__double2loint(tt) & 0xFFu) << (8 * (kk & 3));
     }
-    const int64_t r = r0 + rr, k = k0 + kk;
-    tile[rr][band_col(kk)] = (r < a.rows && k < a.K) ? virtual_elem<double>(a, r, k) : 0.0;
+    *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
-// One band: warp w owns row r0 + w, lane l its K values 16 l .. 16 l + 15 of
-// each K tile.
-__device__ __forceinline__ void oz_pack_band(const PackArgs &a, int64_t r0, double (*tile)[kBandStride]) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t grow = r0 + w;
-  const int64_t kpad = (int64_t)a.kblocks * kKBytes;  // digits written per row (bytes = K values)
-  unsigned long long mb = 0;
-  for (int64_t k0 = 0; k0 < a.K; k0 += kBandK) {
-    load_band<false>(a, r0, k0, tile);
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      const unsigned long long b =
-          (unsigned long long)__double_as_longlong(fabs(tile[w][band_col(lane * 16 + kk)]));
-      mb = b > mb ? b : mb;
+// A walk over this CTA's bands, one tile step at a time: band index
+// b = blockIdx.x + n * gridDim.x, steps 0 .. nk1 + nk2 - 1 per band
+// (nk1 tiles of phase 1, nk2 of phase 2; phase-2 tiles past K load nothing).
+// `Bands` maps a band index to its PackArgs and first row.
+template <class Bands>
+struct BandCursor {
+  int64_t b;
+  int t;
+  const PackArgs *a;
+  int64_t r0;
+  int nk1, nk2;
+  __device__ __forceinline__ void seat(const Bands &bands) {
+    if (b < bands.count()) {
+      a = bands.args(b, r0);
+      nk1 = (int)((a->K + kBandK - 1) / kBandK);
+      nk2 = (int)(((int64_t)a->kblocks * kKBytes + kBandK - 1) / kBandK);
     }
-    __syncthreads();
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long x = __shfl_xor_sync(0xffffffffu, mb, o);
-    mb = x > mb ? x : mb;
-  }
-  // E: the row max's frexp exponent + 1; non-finite rows get kNonFinite,
-  // zero digits and a place on the fixup list.
-  int E = 0;
-  const bool bad = mb >= 0x7FF0000000000000ull;
-  if (bad) {
-    E = kNonFinite;
-  } else if (mb) {
-    frexp(__longlong_as_double((long long)mb), &E);
-    E += 1;
-  }
-  const bool live = grow < a.rows_pad;
-  if (live && lane == 0) {
-    a.exp_out[grow] = E;
-    if (bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
-  }
-  for (int64_t k0 = 0; k0 < kpad; k0 += kBandK) {
-    if (k0 < a.K) load_band<true>(a, r0, k0, tile);
-    __syncthreads();
-    const int64_t kc = k0 + lane * 16;
-    if (live && kc < kpad) {
-      double x[16];
-#pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        const double v = k0 < a.K ? tile[w][band_col(lane * 16 + kk)] : 0.0;
-        x[kk] = (bad || !mb) ? 0.0 : scale2(v, -E);
-      }
-      const int64_t off = panel_tile_base(a, grow, kc);
-      for (int p = 0; p < a.nslices; ++p) {
-        uint32_t wd[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          // y = 254 x; d = y rounded to the nearest integer (ties to even, like
-          // rint) by adding and removing 1.5 * 2^52, whose low word then holds
-          // d in two's complement; x = y - d.  Four full-rate FP64 adds and
-          // multiplies, no rounding or conversion instructions; the _rn
-          // intrinsics keep the compiler from fusing the steps.
-          constexpr double kRound = 6755399441055744.0;
-          const double y = __dmul_rn(x[kk], 254.0);
-          const double t = __dadd_rn(y, kRound);
-          const double d = __dsub_rn(t, kRound);
-          x[kk] = __dsub_rn(y, d);
-          wd[kk >> 2] |= ((uint32_t)__double2loint(t) & 0xFFu) << (8 * (kk & 3));
-        }
-        *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
-      }
+  __device__ __forceinline__ bool valid(const Bands &bands) const { return b < bands.count(); }
+  __device__ __forceinline__ void next(const Bands &bands) {
+    if (++t == nk1 + nk2) {
+      t = 0;
+      b += gridDim.x;
+      seat(bands);
     }
-    __syncthreads();
   }
+};
+
+template <class Bands>
+__device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring) {
+  const uint32_t ring_u32 = smem_u32(ring);
+  constexpr uint32_t kTileBytes = kBandRows * kBandStride * 8;
+  BandCursor<Bands> in{(int64_t)blockIdx.x, 0, nullptr, 0, 0, 0}, out = in;
+  in.seat(bands);
+  out.seat(bands);
+  uint32_t issued = 0, done = 0;
+  auto issue = [&]() {
+    if (in.valid(bands)) {
+      const int64_t k0 = (int64_t)(in.t < in.nk1 ? in.t : in.t - in.nk1) * kBandK;
+      if (k0 < in.a->K) band_issue(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes);
+      in.next(bands);
+    }
+    cp_async_commit();
+    ++issued;
+  };
+  for (int q = 0; q < kPackBufs - 1; ++q) issue();
+  BandState bs{0, 0, false};
+  while (out.valid(bands)) {
+    cp_async_wait<kPackBufs - 2>();  // this step's tile has landed (for this thread)
+    __syncthreads();                 // ... for every thread; the oldest buffer is free again
+    issue();
+    band_process(*out.a, out.r0, out.t, out.nk1, ring + (size_t)(done % kPackBufs) * kBandRows * kBandStride, bs);
+    ++done;
+    out.next(bands);
+  }
+  cp_async_wait<0>();
 }
 
 // Both operands of one plan: bands [0, nbA) of A, then [0, nbB) of B.
-__global__ void __launch_bounds__(256, 2)
-    oz_pack_fused_kernel(PackArgs pa, PackArgs pb, int64_t nbA, int64_t nbB) {
-  __shared__ double tile[kBandRows][kBandStride];
-  for (int64_t b = blockIdx.x; b < nbA + nbB; b += gridDim.x) {
-    if (b < nbA) oz_pack_band(pa, b * kBandRows, tile);
-    else oz_pack_band(pb, (b - nbA) * kBandRows, tile);
+struct PairBands {
+  const PackArgs *pa, *pb;
+  int64_t nbA, nbB;
+  __device__ __forceinline__ int64_t count() const { return nbA + nbB; }
+  __device__ __forceinline__ const PackArgs *args(int64_t b, int64_t &r0) const {
+    if (b < nbA) {
+      r0 = b * kBandRows;
+      return pa;
+    }
+    r0 = (b - nbA) * kBandRows;
+    return pb;
   }
+};
+
+__global__ void __launch_bounds__(256, 2)
+    oz_pack_fused_kernel(const __grid_constant__ PackArgs pa, const __grid_constant__ PackArgs pb, int64_t nbA,
+                         int64_t nbB) {
+  extern __shared__ __align__(16) double pack_ring[];
+  oz_pack_walk(PairBands{&pa, &pb, nbA, nbB}, pack_ring);
 }
 
 // ---------------------------------------------------------------- GEMM ---
@@ -1506,6 +1594,7 @@ int tc_prepare(qs_plan *p) {
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
+    cudaFuncSetAttribute(oz_pack_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
     attr_set[0] = attr_set[1] = true;
   }
   return QS_OK;
@@ -1687,7 +1776,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     if (oz) {
       const int64_t nbA = cdiv(pa.rows_pad, kBandRows), nbB = cdiv(pb.rows_pad, kBandRows);
       const int grid = (int)std::min<int64_t>(nbA + nbB, 2 * (int64_t)num_sms());
-      oz_pack_fused_kernel<<<grid, 256, 0, st>>>(pa, pb, nbA, nbB);
+      oz_pack_fused_kernel<<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
       if (ev) {
         cudaEventRecord(ev[1], st);
         cudaEventRecord(ev[2], st);
@@ -1782,13 +1871,20 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
 }
 
 // The fused pack over every band of every (problem, side) job.
-__global__ void __launch_bounds__(256, 2) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
-  __shared__ double tile[kBandRows][kBandStride];
-  for (int b = blockIdx.x; b < nbands; b += gridDim.x) {
-    const PackJob &j = jobs[pack_job(jobs, njobs, b)];
-    const PackArgs pa = j.pa;
-    oz_pack_band(pa, (int64_t)(b - j.block_start) * kBandRows, tile);
+struct GroupBands {
+  const PackJob *jobs;
+  int njobs, nbands;
+  __device__ __forceinline__ int64_t count() const { return nbands; }
+  __device__ __forceinline__ const PackArgs *args(int64_t b, int64_t &r0) const {
+    const PackJob &j = jobs[pack_job(jobs, njobs, (int)b)];
+    r0 = (b - j.block_start) * kBandRows;
+    return &j.pa;
   }
+};
+
+__global__ void __launch_bounds__(256, 2) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
+  extern __shared__ __align__(16) double pack_ring[];
+  oz_pack_walk(GroupBands{jobs, njobs, nbands}, pack_ring);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
@@ -1918,8 +2014,14 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const ZeroJob *zero = (const ZeroJob *)(d + g.off_zero);
     const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
     const int pgrid = std::min(n, 4 * num_sms());
+    static bool pack_attr = false;
+    if (!pack_attr) {
+      cudaFuncSetAttribute(oz_pack_fused_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
+      pack_attr = true;
+    }
     oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
-    oz_pack_fused_grouped<<<std::min(g.pack_blocks, 2 * num_sms()), 256, 0, st>>>(jobs, g.njobs, g.pack_blocks);
+    oz_pack_fused_grouped<<<std::min(g.pack_blocks, 2 * num_sms()), 256, kPackSmem, st>>>(jobs, g.njobs,
+                                                                                           g.pack_blocks);
     if (g.cls == TC_CLASS_OZ4)
       oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
     else if (g.cls == TC_CLASS_OZ6)

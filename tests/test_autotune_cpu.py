@@ -37,6 +37,7 @@ def fake(times, errs=None, calls=None):
 T64 = {("native", 1, False): 5.0, ("native", 2, False): 4.0, ("native", 3, False): 6.0,
        ("native", 4, False): 7.0, ("native", 5, False): 2.0, ("native", 6, False): 2.5,
        ("native", 7, False): 3.0, ("native", 8, False): 3.5, ("native", 9, False): 3.8,
+       ("native", 10, False): 2.2,
        ("ozaki", 0, False): 1.0, ("ozaki", 0, True): 1.5}
 
 
@@ -47,13 +48,13 @@ def test_picks_fastest_and_caches_on_disk(qs, at, tmp_path):
     C, A, ia, B, ib, ic = views(qs, 300, 200, 260)
     opts = t.options(C, A, ia, B, ib, ic)
     assert opts == {"method": "ozaki"}
-    # SIMT tiles 1-4, DMMA tiles 5-9 (real Float64 operands), two Ozaki variants
-    assert len(calls) == 11 and t.misses == 1
-    assert sorted(c["native_tile"] for c in calls if c["method"] == "native") == list(range(1, 10))
+    # SIMT tiles 1-4, DMMA tiles 5-10 (real Float64 operands), two Ozaki variants
+    assert len(calls) == 12 and t.misses == 1
+    assert sorted(c["native_tile"] for c in calls if c["method"] == "native") == list(range(1, 11))
     # same class (sizes in the same log2 buckets): a hit, no measurement
     C2, A2, _, B2, _, _ = views(qs, 400, 250, 300)
     assert t.options(C2, A2, ia, B2, ib, ic) == {"method": "ozaki"}
-    assert t.hits == 1 and len(calls) == 11
+    assert t.hits == 1 and len(calls) == 12
     # a new process reads the file
     t2 = at.Autotuner(qs, path=path, measure=fake(T64, calls=calls), device_name="B200")
     assert t2.options(C, A, ia, B, ib, ic) == {"method": "ozaki"} and t2.hits == 1

@@ -139,8 +139,7 @@ def test_skinny_path(qs, orc, et, MKN):
 
 def test_small_problem_tiles(qs, orc):
     # The c0 permuted matmul (M = (a,b) = 96*32, N = 80, K = 128).  Real
-    # Float64 operands take the DMMA kernel; a 128x128 grid would leave SMs
-    # idle, so the plan takes 64x64 DMMA tiles.  The SIMT kernel's 32x32
+    # Float64 operands take the DMMA kernel with 64x64 tiles.  The SIMT kernel's 32x32
     # tiles (forced) keep the ScalarKernel FMA order: bitwise equal.
     rng = np.random.default_rng(96)
     A = colmajor_pair(qs, rng, (96, 128, 32), "Float64")
