@@ -274,10 +274,10 @@ __device__ __forceinline__ void oz2_drain_ring(uint64_t *full, int nslots, uint3
   }
 }
 
-// Pair tile t -> (m-pair, n-tile), in bands of kBandM / 2 m-pairs: the same
-// kBandM m-tiles per band as the one-SM kernel, so a wave's panels fit L2.
-__device__ __forceinline__ void pair_tile_coords(int t, int mpairs, int ntiles, int &mp, int &nt) {
-  constexpr int kBand = kBandM / 2;
+// Pair tile t -> (m-pair, n-tile), in bands of band_m / 2 m-pairs: the same
+// m-tiles per band as the one-SM kernel, so a wave's panels fit L2.
+__device__ __forceinline__ void pair_tile_coords(int t, int mpairs, int ntiles, int band_m, int &mp, int &nt) {
+  const int kBand = band_m / 2;
   const int per_band = kBand * ntiles;
   const int band = t / per_band, r = t - band * per_band;
   const int m0 = band * kBand;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(320, 1)
       c.issuedA = c.issuedB = 0;
       for (int pt = cluster; pt < npair_tiles && !a.hold_loads; pt += nclusters) {
         int mp, nt;
-        pair_tile_coords(pt, mpairs, a.ntiles, mp, nt);
+        pair_tile_coords(pt, mpairs, a.ntiles, a.band_m, mp, nt);
         const int mt = 2 * mp + (int)rank;
         const int rowA0 = mt * a.kblocks * 128;
         const int rowB0 = nt * a.kblocks * 128 + (int)rank * 64;
@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(320, 1)
     double sum[64];
     for (int pt = cluster; pt < npair_tiles; pt += nclusters) {
       int mp, nt;
-      pair_tile_coords(pt, mpairs, a.ntiles, mp, nt);
+      pair_tile_coords(pt, mpairs, a.ntiles, a.band_m, mp, nt);
       const int mt = 2 * mp + (int)rank;
       const int64_t m0 = (int64_t)mt * 128, n0 = (int64_t)nt * 128;
       named_bar_sync(1, 256);

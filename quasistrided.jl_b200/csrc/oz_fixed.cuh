@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(320, 1)
         int lt;
         const GemmArgs &P = tile_problem<GROUPED>(a, gt, tile, lt);
         int mt, nt;
-        tile_coords(lt, P.mtiles, P.ntiles, mt, nt);
+        tile_coords(lt, P.mtiles, P.ntiles, P.band_m, mt, nt);
         c.planeA = P.planeA;
         c.planeB = P.planeB;
         const uint8_t *tileA = P.panelA + (int64_t)mt * P.kblocks * TILE;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(320, 1)
       int lt;
       const GemmArgs &Pg = tile_problem<GROUPED>(a, gt, tile, lt);
       int mt, nt;
-      tile_coords(lt, Pg.mtiles, Pg.ntiles, mt, nt);
+      tile_coords(lt, Pg.mtiles, Pg.ntiles, Pg.band_m, mt, nt);
       const int64_t m0 = (int64_t)mt * 128, n0 = (int64_t)nt * 128;
       named_bar_sync(1, 256);
       if (et < 128) {

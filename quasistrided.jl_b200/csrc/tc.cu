@@ -22,6 +22,7 @@
 #include <cudaTypedefs.h>
 
 #include <climits>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <sstream>
@@ -486,7 +487,7 @@ struct GemmArgs {
   double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
   uint64_t wait_ns;  // bound of every barrier wait (qs_plan_set_wait_limit)
   int hold_loads;    // failure-detection test: the producers issue no copies
-  int pad_;
+  int band_m;        // tile raster: m-tiles per band (Ozaki kernels)
 };
 
 // The alpha/beta store of one 16-column chunk of a row of the tile, values
@@ -1268,17 +1269,27 @@ struct OzFixedSched {
   }
 };
 
-// Tile t of a problem -> (mt, nt), in bands of kBandM m-tiles: within a band
-// the n-tiles advance slowest, so the CTAs of one wave share a few A panels
-// and a band's worth of B panels instead of every B panel.
-constexpr int kBandM = 16;
-__device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int &mt, int &nt) {
-  const int per_band = kBandM * ntiles;
+// Tile t of a problem -> (mt, nt), in bands of `band` m-tiles: within a
+// band the n-tiles advance slowest, so the CTAs of one wave share a few A
+// panels and a band's worth of B panels instead of every B panel.
+__device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int band_m, int &mt, int &nt) {
+  const int per_band = band_m * ntiles;
   const int band = t / per_band, r = t - band * per_band;
-  const int m0 = band * kBandM;
-  const int bm = mtiles - m0 < kBandM ? mtiles - m0 : kBandM;
+  const int m0 = band * band_m;
+  const int bm = mtiles - m0 < band_m ? mtiles - m0 : band_m;
   mt = m0 + r % bm;
   nt = r / bm;
+}
+
+// m-tiles per raster band of the Ozaki GEMMs: 16, or QS_OZ_BAND_M (a tuning
+// knob, 2..64) read once per process.
+static int oz_band_m() {
+  static int v = [] {
+    const char *e = std::getenv("QS_OZ_BAND_M");
+    const int x = e ? std::atoi(e) : 0;
+    return x >= 2 && x <= 64 ? x : 16;
+  }();
+  return v;
 }
 
 // Ring slot and phase parity of load l of a block whose first load has
@@ -1684,7 +1695,7 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
   a.wait_ns = p->wait_ns;
   a.hold_loads = p->hold_loads;
-  a.pad_ = 0;
+  a.band_m = oz_band_m();
   return a;
 }
 
