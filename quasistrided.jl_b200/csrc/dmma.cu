@@ -311,16 +311,17 @@ int dmma_shape_mn(int64_t M, int64_t N) {
 
 // The dynamic shared-memory opt-in of one kernel instance, set on the
 // first launch on each device (a per-launch driver call costs microseconds
-// on the one-shot contract path).
-template <class Cfg, class K>
-static cudaError_t dmma_smem_attr(K kernel) {
+// on the one-shot contract path).  KERNEL makes the flag one per kernel:
+// instances of one signature share a function-pointer type.
+template <class Cfg, auto KERNEL>
+static cudaError_t dmma_smem_attr() {
   static std::atomic<uint64_t> done{0};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 63;
   const uint64_t bit = 1ull << dev;
   if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
   const cudaError_t e =
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
+      cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::kSmem);
   if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
   return e;
 }
@@ -334,10 +335,10 @@ static cudaError_t launch_dmma_s(const Operands &op, const Scalars<double> &s, i
   dim3 grid((unsigned)(gm * gn), 1, (unsigned)(op.offBatch ? (op.P < 65535 ? op.P : 65535) : 1));
   cudaError_t e;
   if (op.offBatch) {
-    if ((e = dmma_smem_attr<Cfg>(dmma_gemm_kernel<Cfg, true>)) != cudaSuccess) return e;
+    if ((e = dmma_smem_attr<Cfg, dmma_gemm_kernel<Cfg, true>>()) != cudaSuccess) return e;
     dmma_gemm_kernel<Cfg, true><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast);
   } else {
-    if ((e = dmma_smem_attr<Cfg>(dmma_gemm_kernel<Cfg, false>)) != cudaSuccess) return e;
+    if ((e = dmma_smem_attr<Cfg, dmma_gemm_kernel<Cfg, false>>()) != cudaSuccess) return e;
     dmma_gemm_kernel<Cfg, false><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast);
   }
   return cudaGetLastError();
@@ -359,7 +360,7 @@ cudaError_t launch_dmma(const Operands &op, const double *alpha, const double *b
 template <int SHAPE>
 static cudaError_t dmma_group_launch_s(const void *jobs, int njobs, int blocks, cudaStream_t st) {
   using Cfg = typename DmmaShape<SHAPE>::Cfg;
-  cudaError_t e = dmma_smem_attr<Cfg>(dmma_gemm_grouped_kernel<Cfg>);
+  cudaError_t e = dmma_smem_attr<Cfg, dmma_gemm_grouped_kernel<Cfg>>();
   if (e != cudaSuccess) return e;
   dmma_gemm_grouped_kernel<Cfg>
       <<<blocks, Cfg::kThreads, Cfg::kSmem, st>>>(static_cast<const NativeJob<double> *>(jobs), njobs);

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdlib>
 #include <cmath>
@@ -246,25 +247,92 @@ __device__ __forceinline__ void cp_async_4_8(uint32_t saddr, const void *g, int 
                  : "memory");
 }
 
+// Element kinds of a pack walk, fixed per launch: real Float64 or real
+// Float32 operands take straight-line copies with their row offsets hoisted
+// per band; anything else (complex layouts, mixed types) the general path.
+enum { kPackF64 = 0, kPackF32 = 1, kPackAny = 2 };
+
+__host__ __device__ inline int pack_kind_of(const PackArgs &a) {
+  if (a.cmode == 0 && a.TX == QS_F64) return kPackF64;
+  if (a.cmode == 0 && a.TX == QS_F32) return kPackF32;
+  return kPackAny;
+}
+
+// The issue cursor's row offsets (element index of column 0 of each row the
+// thread copies; INT64_MIN outside the operand): rfast threads use ro[0]
+// (their one row), K-fast threads all kBandRows rows.
+struct IssueRows {
+  int64_t ro[kBandRows];
+};
+
+template <int KIND>
+__device__ __forceinline__ void band_seat_rows(const PackArgs &a, int64_t r0, IssueRows &ir) {
+  if constexpr (KIND != kPackAny) {
+    if (a.rfast) {
+      const int64_t r = r0 + threadIdx.x % kBandRows;
+      ir.ro[0] = r < a.rows ? a.Xbase + __ldg(a.offR + r) : INT64_MIN;
+    } else {
+#pragma unroll
+      for (int rr = 0; rr < kBandRows; ++rr) {
+        const int64_t r = r0 + rr;
+        ir.ro[rr] = r < a.rows ? a.Xbase + __ldg(a.offR + r) : INT64_MIN;
+      }
+    }
+  }
+}
+
 // Issue the copies of K tile [k0, k0 + kBandK) of virtual rows
 // [r0, r0 + kBandRows) into `tile` (slot (row, k) at row * kBandStride +
-// band_col(k)), zero-filled outside the operand.  Real operands (cmode 0):
-// slot = element.  1r (cmode 2, K doubled): slots 2j, 2j+1 = re, im of
-// complex K index j.  1e (cmode 1, rows and K doubled): complex row i goes
-// to even row 2i as in 1r; odd rows are formed from it on read.  A real
-// operand in a complex layout gets zero imaginary slots.
-__device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_t k0, uint32_t tile) {
+// band_col(k)), zero-filled outside the operand, coalesced along X's
+// unit-stride axis.  Real operands: slot = element.  General path: 1r
+// (cmode 2, K doubled): slots 2j, 2j+1 = re, im of complex K index j; 1e
+// (cmode 1, rows and K doubled): complex row i goes to even row 2i as in 1r
+// and odd rows are formed from it on read; a real operand in a complex
+// layout gets zero imaginary slots.
+template <int KIND>
+__device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_t k0, uint32_t tile,
+                                           const IssueRows &ir) {
   const int tid = threadIdx.x;
+  const char *X = static_cast<const char *>(a.X);
+  if constexpr (KIND != kPackAny) {
+    constexpr int ESZ = KIND == kPackF64 ? 8 : 4;
+    if (a.rfast) {
+      const int rr = tid % kBandRows, kb = tid / kBandRows;
+      const int64_t ro = ir.ro[0];
+#pragma unroll
+      for (int i = 0; i < kBandK / (256 / kBandRows); ++i) {
+        const int kk = kb + (256 / kBandRows) * i;
+        const int64_t k = k0 + kk;
+        const bool ok = ro != INT64_MIN && k < a.K;
+        const char *src = ok ? X + (ro + __ldg(a.offK + k)) * ESZ : X;
+        cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < kBandK / 256; ++h) {
+        const int kk = tid + 256 * h;
+        const int64_t k = k0 + kk;
+        const bool kok = k < a.K;
+        const int64_t ko = kok ? __ldg(a.offK + k) : 0;
+#pragma unroll
+        for (int rr = 0; rr < kBandRows; ++rr) {
+          const bool ok = kok && ir.ro[rr] != INT64_MIN;
+          const char *src = ok ? X + (ir.ro[rr] + ko) * ESZ : X;
+          cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
+        }
+      }
+    }
+    return;
+  }
   const bool cx = a.TX == QS_C32 || a.TX == QS_C64;
   const int esz = (a.TX == QS_F64 || a.TX == QS_C64) ? 8 : 4;
-  const char *X = static_cast<const char *>(a.X);
   auto slot = [&](int rr, int kk) {
     const int64_t r = r0 + rr, k = k0 + kk;
     const uint32_t dst = tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk));
     if (a.cmode == 1 && (rr & 1)) return;  // derived from the even row
     bool ok = r < a.rows && k < a.K;
-    int64_t rix = a.cmode == 1 ? (r >> 1) : r, kix = a.cmode ? (k >> 1) : k;
-    int part = a.cmode ? (int)(k & 1) : 0;
+    const int64_t rix = a.cmode == 1 ? (r >> 1) : r, kix = a.cmode ? (k >> 1) : k;
+    const int part = a.cmode ? (int)(k & 1) : 0;
     if (part && !cx) ok = false;  // imaginary part of a real operand
     const char *src = X;
     if (ok) {
@@ -283,24 +351,31 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
   }
 }
 
-// Virtual value (row w, K index kk) of a staged tile; k0 + kk >= K reads 0.
-__device__ __forceinline__ double band_raw(const PackArgs &a, const double *tile, int row, int kk) {
-  const double *p = tile + row * kBandStride + band_col(kk);
-  if (a.TX == QS_F64 || a.TX == QS_C64) return *p;
-  return (double)*reinterpret_cast<const float *>(p);
-}
+// Virtual value (row w, K index kk) of a staged tile.
+template <int KIND>
 __device__ __forceinline__ double band_value(const PackArgs &a, const double *tile, int w, int kk) {
-  if (a.cmode == 0) return band_raw(a, tile, w, kk);
-  if (a.cmode == 2) {
-    const double v = band_raw(a, tile, w, kk);
-    return ((kk & 1) && a.conj) ? -v : v;
+  auto raw = [&](int row, int k) -> double {
+    const double *p = tile + row * kBandStride + band_col(k);
+    if constexpr (KIND == kPackF64) return *p;
+    if constexpr (KIND == kPackF32) return (double)*reinterpret_cast<const float *>(p);
+    if (a.TX == QS_F64 || a.TX == QS_C64) return *p;
+    return (double)*reinterpret_cast<const float *>(p);
+  };
+  if constexpr (KIND != kPackAny) {
+    return raw(w, kk);
+  } else {
+    if (a.cmode == 0) return raw(w, kk);
+    if (a.cmode == 2) {
+      const double v = raw(w, kk);
+      return ((kk & 1) && a.conj) ? -v : v;
+    }
+    const int base = w & ~1;
+    const double re = raw(base, kk & ~1);
+    double im = raw(base, kk | 1);
+    if (a.conj) im = -im;
+    const int rp = w & 1, kp = kk & 1;
+    return rp == kp ? re : (rp ? im : -im);
   }
-  const int base = w & ~1;
-  const double re = band_raw(a, tile, base, kk & ~1);
-  double im = band_raw(a, tile, base, kk | 1);
-  if (a.conj) im = -im;
-  const int rp = w & 1, kp = kk & 1;
-  return rp == kp ? re : (rp ? im : -im);
 }
 
 // One row band's state for the processing side.
@@ -312,17 +387,18 @@ struct BandState {
 
 // Process tile `t` (phase 1: t < nk1; phase 2 otherwise) of the band at
 // r0: warp w owns virtual row r0 + w, lane l its K values 16 l .. 16 l + 15.
+// Loaded tiles are zero-filled past K; phase-2 tiles past K are not loaded
+// and read as zeros.
+template <int KIND>
 __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int t, int nk1, const double *tile,
                                              BandState &bs) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t grow = r0 + w;
   if (t < nk1) {
-    const int64_t k0 = (int64_t)t * kBandK;
     if (t == 0) bs.mb = 0;
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
-      const int k = lane * 16 + kk;
-      const double v = k0 + k < a.K ? band_value(a, tile, w, k) : 0.0;
+      const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
       const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
       bs.mb = b > bs.mb ? b : bs.mb;
     }
@@ -353,13 +429,10 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   const int64_t kpad = (int64_t)a.kblocks * kKBytes;  // digits per row (bytes = K values)
   const int64_t kc = k0 + lane * 16;
   if (grow >= a.rows_pad || kc >= kpad) return;
+  const bool zero = bs.bad || !bs.mb || k0 >= a.K;
   double x[16];
 #pragma unroll
-  for (int kk = 0; kk < 16; ++kk) {
-    const int k = lane * 16 + kk;
-    const double v = k0 + k < a.K ? band_value(a, tile, w, k) : 0.0;
-    x[kk] = (bs.bad || !bs.mb) ? 0.0 : scale2(v, -bs.E);
-  }
+  for (int kk = 0; kk < 16; ++kk) x[kk] = zero ? 0.0 : scale2(band_value<KIND>(a, tile, w, lane * 16 + kk), -bs.E);
   const int64_t off = panel_tile_base(a, grow, kc);
   for (int p = 0; p < a.nslices; ++p) {
     uint32_t wd[4] = {0, 0, 0, 0};
@@ -400,28 +473,31 @@ struct BandCursor {
     }
   }
   __device__ __forceinline__ bool valid(const Bands &bands) const { return b < bands.count(); }
-  __device__ __forceinline__ void next(const Bands &bands) {
-    if (++t == nk1 + nk2) {
-      t = 0;
-      b += gridDim.x;
-      seat(bands);
-    }
+  // Advances one step; true when it moved to a new band.
+  __device__ __forceinline__ bool next(const Bands &bands) {
+    if (++t < nk1 + nk2) return false;
+    t = 0;
+    b += gridDim.x;
+    seat(bands);
+    return true;
   }
 };
 
-template <class Bands>
+template <int KIND, class Bands>
 __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring) {
   const uint32_t ring_u32 = smem_u32(ring);
   constexpr uint32_t kTileBytes = kBandRows * kBandStride * 8;
   BandCursor<Bands> in{(int64_t)blockIdx.x, 0, nullptr, 0, 0, 0}, out = in;
   in.seat(bands);
   out.seat(bands);
+  IssueRows ir;
+  if (in.valid(bands)) band_seat_rows<KIND>(*in.a, in.r0, ir);
   uint32_t issued = 0, done = 0;
   auto issue = [&]() {
     if (in.valid(bands)) {
       const int64_t k0 = (int64_t)(in.t < in.nk1 ? in.t : in.t - in.nk1) * kBandK;
-      if (k0 < in.a->K) band_issue(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes);
-      in.next(bands);
+      if (k0 < in.a->K) band_issue<KIND>(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes, ir);
+      if (in.next(bands) && in.valid(bands)) band_seat_rows<KIND>(*in.a, in.r0, ir);
     }
     cp_async_commit();
     ++issued;
@@ -432,7 +508,8 @@ __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring) {
     cp_async_wait<kPackBufs - 2>();  // this step's tile has landed (for this thread)
     __syncthreads();                 // ... for every thread; the oldest buffer is free again
     issue();
-    band_process(*out.a, out.r0, out.t, out.nk1, ring + (size_t)(done % kPackBufs) * kBandRows * kBandStride, bs);
+    band_process<KIND>(*out.a, out.r0, out.t, out.nk1,
+                       ring + (size_t)(done % kPackBufs) * kBandRows * kBandStride, bs);
     ++done;
     out.next(bands);
   }
@@ -454,11 +531,46 @@ struct PairBands {
   }
 };
 
+template <int KIND>
 __global__ void __launch_bounds__(256, 2)
     oz_pack_fused_kernel(const __grid_constant__ PackArgs pa, const __grid_constant__ PackArgs pb, int64_t nbA,
                          int64_t nbB) {
   extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk(PairBands{&pa, &pb, nbA, nbB}, pack_ring);
+  oz_pack_walk<KIND>(PairBands{&pa, &pb, nbA, nbB}, pack_ring);
+}
+
+// The kind both operands share, else the general path.
+static int pack_kind(const PackArgs &pa, const PackArgs &pb) {
+  const int ka = pack_kind_of(pa), kb = pack_kind_of(pb);
+  return ka == kb ? ka : kPackAny;
+}
+
+template <class K>
+static void pack_smem_attr(K kernel, std::atomic<int> &done) {
+  if (!done.load()) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
+    done.store(1);
+  }
+}
+
+static cudaError_t launch_pack_fused(const PackArgs &pa, const PackArgs &pb, int64_t nbA, int64_t nbB, int grid,
+                                     cudaStream_t st) {
+  static std::atomic<int> done[3];
+  switch (pack_kind(pa, pb)) {
+    case kPackF64:
+      pack_smem_attr(oz_pack_fused_kernel<kPackF64>, done[0]);
+      oz_pack_fused_kernel<kPackF64><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      break;
+    case kPackF32:
+      pack_smem_attr(oz_pack_fused_kernel<kPackF32>, done[1]);
+      oz_pack_fused_kernel<kPackF32><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      break;
+    default:
+      pack_smem_attr(oz_pack_fused_kernel<kPackAny>, done[2]);
+      oz_pack_fused_kernel<kPackAny><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      break;
+  }
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- GEMM ---
@@ -1605,7 +1717,6 @@ int tc_prepare(qs_plan *p) {
                          (int)oz_smem_bytes());
     cudaFuncSetAttribute(oz_gemm_pair_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)oz_smem_bytes());
-    cudaFuncSetAttribute(oz_pack_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
     attr_set[0] = attr_set[1] = true;
   }
   return QS_OK;
@@ -1787,7 +1898,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     if (oz) {
       const int64_t nbA = cdiv(pa.rows_pad, kBandRows), nbB = cdiv(pb.rows_pad, kBandRows);
       const int grid = (int)std::min<int64_t>(nbA + nbB, 2 * (int64_t)num_sms());
-      oz_pack_fused_kernel<<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      launch_pack_fused(pa, pb, nbA, nbB, grid, st);
       if (ev) {
         cudaEventRecord(ev[1], st);
         cudaEventRecord(ev[2], st);
@@ -1893,9 +2004,10 @@ struct GroupBands {
   }
 };
 
+template <int KIND>
 __global__ void __launch_bounds__(256, 2) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
   extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk(GroupBands{jobs, njobs, nbands}, pack_ring);
+  oz_pack_walk<KIND>(GroupBands{jobs, njobs, nbands}, pack_ring);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
@@ -1962,6 +2074,12 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   }
   g.njobs = (int)jobs.size();
   g.pack_blocks = blocks;
+  g.pack_kind = kPackAny;
+  if (oz && !jobs.empty()) {
+    g.pack_kind = pack_kind_of(jobs[0].pa);
+    for (const PackJob &j : jobs)
+      if (pack_kind_of(j.pa) != g.pack_kind) g.pack_kind = kPackAny;
+  }
   g.tiles = tiles.back();
   size_t off = 0;
   g.off_pack = off;
@@ -2025,14 +2143,23 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const ZeroJob *zero = (const ZeroJob *)(d + g.off_zero);
     const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
     const int pgrid = std::min(n, 4 * num_sms());
-    static bool pack_attr = false;
-    if (!pack_attr) {
-      cudaFuncSetAttribute(oz_pack_fused_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
-      pack_attr = true;
-    }
     oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
-    oz_pack_fused_grouped<<<std::min(g.pack_blocks, 2 * num_sms()), 256, kPackSmem, st>>>(jobs, g.njobs,
-                                                                                           g.pack_blocks);
+    static std::atomic<int> done[3];
+    const int pgrid2 = std::min(g.pack_blocks, 2 * num_sms());
+    switch (g.pack_kind) {
+      case kPackF64:
+        pack_smem_attr(oz_pack_fused_grouped<kPackF64>, done[0]);
+        oz_pack_fused_grouped<kPackF64><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        break;
+      case kPackF32:
+        pack_smem_attr(oz_pack_fused_grouped<kPackF32>, done[1]);
+        oz_pack_fused_grouped<kPackF32><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        break;
+      default:
+        pack_smem_attr(oz_pack_fused_grouped<kPackAny>, done[2]);
+        oz_pack_fused_grouped<kPackAny><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        break;
+    }
     if (g.cls == TC_CLASS_OZ4)
       oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
     else if (g.cls == TC_CLASS_OZ6)
