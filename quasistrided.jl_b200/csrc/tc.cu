@@ -600,6 +600,8 @@ struct GemmArgs {
   uint64_t wait_ns;  // bound of every barrier wait (qs_plan_set_wait_limit)
   int hold_loads;    // failure-detection test: the producers issue no copies
   int band_m;        // tile raster: m-tiles per band (Ozaki kernels)
+  int c_stream;      // Float64 C loads/stores with the evict-first hint
+  int pad_;
 };
 
 // The alpha/beta store of one 16-column chunk of a row of the tile, values
@@ -724,7 +726,7 @@ __device__ __forceinline__ void store_chunk_f64(const GemmArgs &a, const double 
     for (int e = 0; e < G; ++e) {
       const int jj = 16 * c + e0 + e;
       const bool ok = row_store && n0 + jj < a.N && s_expN[jj] != kNF;
-      old[e] = (ok && bc != 0) ? C[crow + s_offN[jj]] : 0.0;
+      old[e] = (ok && bc != 0) ? (a.c_stream ? __ldcs(C + crow + s_offN[jj]) : C[crow + s_offN[jj]]) : 0.0;
     }
 #pragma unroll
     for (int e = 0; e < G; ++e) {
@@ -736,7 +738,8 @@ __device__ __forceinline__ void store_chunk_f64(const GemmArgs &a, const double 
       if (bc == 0) r = al * x;
       else if (bc == 1) r = fma(al, x, old[e]);
       else r = fma(al, x, be * old[e]);
-      C[crow + s_offN[jj]] = r;
+      if (a.c_stream) __stcs(C + crow + s_offN[jj], r);
+      else C[crow + s_offN[jj]] = r;
     }
   }
 }
@@ -1393,6 +1396,16 @@ __device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int b
   nt = r / bm;
 }
 
+// Whether the Ozaki epilogue's Float64 C traffic carries the evict-first
+// hint (QS_OZ_C_STREAM=1; a tuning knob read once per process).
+static int oz_c_stream() {
+  static int v = [] {
+    const char *e = std::getenv("QS_OZ_C_STREAM");
+    return e && std::atoi(e) == 1 ? 1 : 0;
+  }();
+  return v;
+}
+
 // m-tiles per raster band of the Ozaki GEMMs: 16, or QS_OZ_BAND_M (a tuning
 // knob, 2..64) read once per process.
 static int oz_band_m() {
@@ -1807,6 +1820,8 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.wait_ns = p->wait_ns;
   a.hold_loads = p->hold_loads;
   a.band_m = oz_band_m();
+  a.c_stream = oz_c_stream();
+  a.pad_ = 0;
   return a;
 }
 
