@@ -28,6 +28,7 @@
 #include <atomic>
 #include <climits>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -111,7 +112,8 @@ __device__ __forceinline__ void dmma_gather(const double *X, const int64_t *rowo
 // dynamic shared memory (Cfg::kSmem bytes).
 template <class Cfg>
 __device__ __forceinline__ void dmma_gemm_tile(const Operands &op, const Scalars<double> &s, int a_mfast,
-                                               int b_nfast, int64_t tm, int64_t tn, double *smem) {
+                                               int b_nfast, int64_t tm, int64_t tn, double *smem,
+                                               bool s_stream = false) {
   constexpr int BM = Cfg::BM, BN = Cfg::BN, STAGES = Cfg::STAGES, MI = Cfg::MI, NJ = Cfg::NJ;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tig = lane & 3;
@@ -210,16 +212,23 @@ __device__ __forceinline__ void dmma_gemm_tile(const Operands &op, const Scalars
         for (int c = 0; c < 2; ++c) {
           if (cn[j][c] == INT64_MIN) continue;
           const int64_t idx = cm + cn[j][c];
-          const double old = s.beta_case == 0 ? 0.0 : load_c<double>(op.C, idx, op.TC);
-          store_c<double>(op.C, idx, op.TC, axpby(s, acc[i][j][2 * h + c], old));
+          if (s_stream && op.TC == QS_F64) {
+            // evict-first: C streams through L2 without displacing A and B
+            double *Cd = static_cast<double *>(op.C) + idx;
+            const double old = s.beta_case == 0 ? 0.0 : __ldcs(Cd);
+            __stcs(Cd, axpby(s, acc[i][j][2 * h + c], old));
+          } else {
+            const double old = s.beta_case == 0 ? 0.0 : load_c<double>(op.C, idx, op.TC);
+            store_c<double>(op.C, idx, op.TC, axpby(s, acc[i][j][2 * h + c], old));
+          }
         }
     }
 }
 
-// Tiles in bands of 8 M tiles, N tiles within a band: a wave of CTAs shares
-// few A and B panels in L2.
-__device__ __forceinline__ void dmma_band(int64_t b, int64_t gm, int64_t gn, int64_t &tm, int64_t &tn) {
-  constexpr int64_t kBand = 8;
+// Tiles in bands of `kBand` M tiles, N tiles within a band: a wave of CTAs
+// shares few A and B panels in L2.
+__device__ __forceinline__ void dmma_band(int64_t b, int64_t gm, int64_t gn, int64_t kBand, int64_t &tm,
+                                          int64_t &tn) {
   const int64_t per = kBand * gn;
   const int64_t band = b / per, r = b - band * per;
   const int64_t rows = (band + 1) * kBand <= gm ? kBand : gm - band * kBand;
@@ -229,16 +238,17 @@ __device__ __forceinline__ void dmma_band(int64_t b, int64_t gm, int64_t gn, int
 
 template <class Cfg, bool BATCHED>
 __global__ void __launch_bounds__(Cfg::kThreads, 1)
-    dmma_gemm_kernel(const __grid_constant__ Operands op, const Scalars<double> s, int a_mfast, int b_nfast) {
+    dmma_gemm_kernel(const __grid_constant__ Operands op, const Scalars<double> s, int a_mfast, int b_nfast,
+                     int band) {
   extern __shared__ __align__(128) double dsm[];
   const int64_t gm = (op.M + Cfg::BM - 1) / Cfg::BM, gn = (op.N + Cfg::BN - 1) / Cfg::BN;
   int64_t tm, tn;
-  dmma_band(blockIdx.x, gm, gn, tm, tn);
+  dmma_band(blockIdx.x, gm, gn, band < 0 ? -band : band, tm, tn);
   if constexpr (!BATCHED) {
     dmma_gemm_tile<Cfg>(op, s, a_mfast, b_nfast, tm, tn, dsm);
   } else {
     for (int64_t b = blockIdx.z; b < op.P; b += gridDim.z) {
-      dmma_gemm_tile<Cfg>(batch_entry(op, b), s, a_mfast, b_nfast, tm, tn, dsm);
+      dmma_gemm_tile<Cfg>(batch_entry(op, b), s, a_mfast, b_nfast, tm, tn, dsm, band < 0);
       __syncthreads();  // the next entry reuses the shared tiles
     }
   }
@@ -291,6 +301,20 @@ void dmma_tile_dims(int shape, int *bm, int *bn) {
   }
 }
 
+// M tiles per raster band (QS_DMMA_BAND_M, a tuning knob, 2..128; default
+// 8), negated when QS_DMMA_C_STREAM=1 asks for evict-first Float64 C
+// traffic.  Read once per process.
+static int dmma_band_m() {
+  static int v = [] {
+    const char *e = std::getenv("QS_DMMA_BAND_M");
+    int x = e ? std::atoi(e) : 0;
+    if (x < 2 || x > 128) x = 8;
+    const char *c = std::getenv("QS_DMMA_C_STREAM");
+    return (c && std::atoi(c) == 1) ? -x : x;
+  }();
+  return v;
+}
+
 bool dmma_eligible(int T, int TA, int TB) { return T == QS_F64 && TA == QS_F64 && TB == QS_F64; }
 
 // By N: 64 x 64 tiles (4 warps, three CTAs per SM) for N > 32 -- on the
@@ -336,10 +360,10 @@ static cudaError_t launch_dmma_s(const Operands &op, const Scalars<double> &s, i
   cudaError_t e;
   if (op.offBatch) {
     if ((e = dmma_smem_attr<Cfg, dmma_gemm_kernel<Cfg, true>>()) != cudaSuccess) return e;
-    dmma_gemm_kernel<Cfg, true><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast);
+    dmma_gemm_kernel<Cfg, true><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast, dmma_band_m());
   } else {
     if ((e = dmma_smem_attr<Cfg, dmma_gemm_kernel<Cfg, false>>()) != cudaSuccess) return e;
-    dmma_gemm_kernel<Cfg, false><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast);
+    dmma_gemm_kernel<Cfg, false><<<grid, Cfg::kThreads, Cfg::kSmem, st>>>(op, s, a_mfast, b_nfast, dmma_band_m());
   }
   return cudaGetLastError();
 }
