@@ -232,7 +232,9 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 // tile slot holds one real value or one complex component (Float32 in its
 // low four bytes), and the virtual matrix (type conversion, conj, the 1e /
 // 1r complex layouts) is formed when a slot is read.
-constexpr int kBandRows = 8, kBandK = 512, kPackBufs = 3;
+constexpr int kBandRows = 4, kBandK = 512, kPackBufs = 3;
+constexpr int kPackThreads = 32 * kBandRows;  // a warp per row
+constexpr int kPackCtasPerSm = 4;
 constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 slot per 16, +4 per row: conflict-free
 constexpr size_t kPackSmem = (size_t)kPackBufs * kBandRows * kBandStride * 8;
 
@@ -300,8 +302,8 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
       const int rr = tid % kBandRows, kb = tid / kBandRows;
       const int64_t ro = ir.ro[0];
 #pragma unroll
-      for (int i = 0; i < kBandK / (256 / kBandRows); ++i) {
-        const int kk = kb + (256 / kBandRows) * i;
+      for (int i = 0; i < kBandK / (kPackThreads / kBandRows); ++i) {
+        const int kk = kb + (kPackThreads / kBandRows) * i;
         const int64_t k = k0 + kk;
         const bool ok = ro != INT64_MIN && k < a.K;
         const char *src = ok ? X + (ro + __ldg(a.offK + k)) * ESZ : X;
@@ -309,8 +311,8 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
       }
     } else {
 #pragma unroll
-      for (int h = 0; h < kBandK / 256; ++h) {
-        const int kk = tid + 256 * h;
+      for (int h = 0; h < kBandK / kPackThreads; ++h) {
+        const int kk = tid + kPackThreads * h;
         const int64_t k = k0 + kk;
         const bool kok = k < a.K;
         const int64_t ko = kok ? __ldg(a.offK + k) : 0;
@@ -341,13 +343,13 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
     }
     cp_async_4_8(dst, src, esz, ok);
   };
-  constexpr int PER = kBandRows * kBandK / 256;
+  constexpr int PER = kBandRows * kBandK / kPackThreads;
   if (a.rfast) {
 #pragma unroll 4
-    for (int i = 0; i < PER; ++i) slot(tid % kBandRows, tid / kBandRows + (256 / kBandRows) * i);
+    for (int i = 0; i < PER; ++i) slot(tid % kBandRows, tid / kBandRows + (kPackThreads / kBandRows) * i);
   } else {
 #pragma unroll 4
-    for (int i = 0; i < PER; ++i) slot(i % kBandRows, tid + 256 * (i / kBandRows));
+    for (int i = 0; i < PER; ++i) slot(i % kBandRows, tid + kPackThreads * (i / kBandRows));
   }
 }
 
@@ -532,7 +534,7 @@ struct PairBands {
 };
 
 template <int KIND>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
     oz_pack_fused_kernel(const __grid_constant__ PackArgs pa, const __grid_constant__ PackArgs pb, int64_t nbA,
                          int64_t nbB) {
   extern __shared__ __align__(16) double pack_ring[];
@@ -559,15 +561,15 @@ static cudaError_t launch_pack_fused(const PackArgs &pa, const PackArgs &pb, int
   switch (pack_kind(pa, pb)) {
     case kPackF64:
       pack_smem_attr(oz_pack_fused_kernel<kPackF64>, done[0]);
-      oz_pack_fused_kernel<kPackF64><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_pack_fused_kernel<kPackF64><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
       break;
     case kPackF32:
       pack_smem_attr(oz_pack_fused_kernel<kPackF32>, done[1]);
-      oz_pack_fused_kernel<kPackF32><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_pack_fused_kernel<kPackF32><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
       break;
     default:
       pack_smem_attr(oz_pack_fused_kernel<kPackAny>, done[2]);
-      oz_pack_fused_kernel<kPackAny><<<grid, 256, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_pack_fused_kernel<kPackAny><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
       break;
   }
   return cudaGetLastError();
@@ -1912,7 +1914,7 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
     const int64_t nA = (int64_t)nrbA * g.kblocks, nB = (int64_t)nrbB * g.kblocks;
     if (oz) {
       const int64_t nbA = cdiv(pa.rows_pad, kBandRows), nbB = cdiv(pb.rows_pad, kBandRows);
-      const int grid = (int)std::min<int64_t>(nbA + nbB, 2 * (int64_t)num_sms());
+      const int grid = (int)std::min<int64_t>(nbA + nbB, kPackCtasPerSm * (int64_t)num_sms());
       launch_pack_fused(pa, pb, nbA, nbB, grid, st);
       if (ev) {
         cudaEventRecord(ev[1], st);
@@ -2020,7 +2022,7 @@ struct GroupBands {
 };
 
 template <int KIND>
-__global__ void __launch_bounds__(256, 2) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
+__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
   extern __shared__ __align__(16) double pack_ring[];
   oz_pack_walk<KIND>(GroupBands{jobs, njobs, nbands}, pack_ring);
 }
@@ -2160,19 +2162,19 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const int pgrid = std::min(n, 4 * num_sms());
     oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
     static std::atomic<int> done[3];
-    const int pgrid2 = std::min(g.pack_blocks, 2 * num_sms());
+    const int pgrid2 = std::min(g.pack_blocks, kPackCtasPerSm * num_sms());
     switch (g.pack_kind) {
       case kPackF64:
         pack_smem_attr(oz_pack_fused_grouped<kPackF64>, done[0]);
-        oz_pack_fused_grouped<kPackF64><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
       case kPackF32:
         pack_smem_attr(oz_pack_fused_grouped<kPackF32>, done[1]);
-        oz_pack_fused_grouped<kPackF32><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
       default:
         pack_smem_attr(oz_pack_fused_grouped<kPackAny>, done[2]);
-        oz_pack_fused_grouped<kPackAny><<<pgrid2, 256, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
     }
     if (g.cls == TC_CLASS_OZ4)
