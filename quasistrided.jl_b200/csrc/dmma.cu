@@ -75,25 +75,17 @@ __device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4]
 template <int R, int PER, int THREADS>
 __device__ __forceinline__ void dmma_gather(const double *X, const int64_t *rowoff, const int64_t *offK,
                                             int64_t k0, int64_t K, int rfast, uint32_t tile) {
-  static_assert((THREADS / 32) * PER == R / 2, "row-fast gather covers the tile");
+  static_assert(THREADS % R == 0 ? (THREADS / R) * PER == 16 : false, "row-fast gather covers the K tile");
   static_assert((THREADS / 16) * PER == R, "K-fast gather covers the rows");
   const int tid = threadIdx.x;
   if (rfast) {
-    // A warp takes 8 consecutive rows (64 contiguous bytes per K index) x 4
-    // K indices {k, k+4, k+1, k+5}: with the row swizzle its 32 eight-byte
-    // writes cover all 16 bank pairs of a row, so a warp's copy lands in the
-    // minimum two shared-memory wavefronts (32 consecutive rows of one K
-    // index put four writes on each bank pair).
-    static_assert(R % 8 == 0 && THREADS % 32 == 0, "row-fast gather groups");
-    constexpr int RGROUPS = R / 8;
-    const int lane = tid & 31;
+    // consecutive threads take consecutive rows; K steps by THREADS / R
+    constexpr int KSTEP = THREADS / R;
+    const int r = tid % R, kb = tid / R;
+    const int64_t ro = rowoff[r];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-      const int slot = (tid >> 5) + (THREADS / 32) * j;  // 0 .. R / 2 - 1
-      const int r = (slot % RGROUPS) * 8 + (lane & 7);
-      const int kq = slot / RGROUPS;                      // 0 .. 3
-      const int k = ((kq & 1) << 1) + ((kq >> 1) << 3) + (((lane >> 3) & 1) << 2) + (lane >> 4);
-      const int64_t ro = rowoff[r];
+      const int k = kb + KSTEP * j;
       const int64_t kg = k0 + k;
       const bool ok = ro != INT64_MIN && kg < K;
       const double *src = ok ? X + ro + __ldg(offK + kg) : X;
