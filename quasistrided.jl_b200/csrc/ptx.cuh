@@ -106,9 +106,11 @@ __device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes) 
 // ------------------------------------------------------------ cp.async ---
 // Per-thread asynchronous global -> shared copies of 4, 8 or 16 bytes
 // (src-size 0 zero-fills), grouped with commit/wait.
+// The copies carry no "memory" clobber, so the compiler may keep loaded
+// values in registers across them; cp_async_wait and __syncthreads, which
+// do clobber memory, order the shared-memory reads of the landed data.
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g, int bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes)
-               : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>

@@ -240,13 +240,12 @@ constexpr size_t kPackSmem = (size_t)kPackBufs * kBandRows * kBandStride * 8;
 
 __device__ __forceinline__ int band_col(int k) { return k + (k >> 4); }
 
+// No "memory" clobber (as cp_async8): loop-invariant loads stay in registers.
 __device__ __forceinline__ void cp_async_4_8(uint32_t saddr, const void *g, int size, bool ok) {
   if (size == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 8 : 0)
-                 : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 8 : 0));
   else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 4 : 0)
-                 : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 4 : 0));
 }
 
 // Element kinds of a pack walk, fixed per launch: real Float64 or real
@@ -296,6 +295,8 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
                                            const IssueRows &ir) {
   const int tid = threadIdx.x;
   const char *X = static_cast<const char *>(a.X);
+  const int64_t K = a.K;
+  const int64_t *__restrict__ offK = a.offK;
   if constexpr (KIND != kPackAny) {
     constexpr int ESZ = KIND == kPackF64 ? 8 : 4;
     if (a.rfast) {
@@ -305,8 +306,8 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
       for (int i = 0; i < kBandK / (kPackThreads / kBandRows); ++i) {
         const int kk = kb + (kPackThreads / kBandRows) * i;
         const int64_t k = k0 + kk;
-        const bool ok = ro != INT64_MIN && k < a.K;
-        const char *src = ok ? X + (ro + __ldg(a.offK + k)) * ESZ : X;
+        const bool ok = ro != INT64_MIN && k < K;
+        const char *src = ok ? X + (ro + __ldg(offK + k)) * ESZ : X;
         cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
       }
     } else {
@@ -314,8 +315,8 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
       for (int h = 0; h < kBandK / kPackThreads; ++h) {
         const int kk = tid + kPackThreads * h;
         const int64_t k = k0 + kk;
-        const bool kok = k < a.K;
-        const int64_t ko = kok ? __ldg(a.offK + k) : 0;
+        const bool kok = k < K;
+        const int64_t ko = kok ? __ldg(offK + k) : 0;
 #pragma unroll
         for (int rr = 0; rr < kBandRows; ++rr) {
           const bool ok = kok && ir.ro[rr] != INT64_MIN;
@@ -328,17 +329,20 @@ __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_
   }
   const bool cx = a.TX == QS_C32 || a.TX == QS_C64;
   const int esz = (a.TX == QS_F64 || a.TX == QS_C64) ? 8 : 4;
+  const int cmode = a.cmode;
+  const int64_t rows = a.rows, Xbase = a.Xbase;
+  const int64_t *__restrict__ offR = a.offR;
   auto slot = [&](int rr, int kk) {
     const int64_t r = r0 + rr, k = k0 + kk;
     const uint32_t dst = tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk));
-    if (a.cmode == 1 && (rr & 1)) return;  // derived from the even row
-    bool ok = r < a.rows && k < a.K;
-    const int64_t rix = a.cmode == 1 ? (r >> 1) : r, kix = a.cmode ? (k >> 1) : k;
-    const int part = a.cmode ? (int)(k & 1) : 0;
+    if (cmode == 1 && (rr & 1)) return;  // derived from the even row
+    bool ok = r < rows && k < K;
+    const int64_t rix = cmode == 1 ? (r >> 1) : r, kix = cmode ? (k >> 1) : k;
+    const int part = cmode ? (int)(k & 1) : 0;
     if (part && !cx) ok = false;  // imaginary part of a real operand
     const char *src = X;
     if (ok) {
-      const int64_t e = a.Xbase + __ldg(a.offR + rix) + __ldg(a.offK + kix);
+      const int64_t e = Xbase + __ldg(offR + rix) + __ldg(offK + kix);
       src = X + (cx ? (2 * e + part) : e) * esz;
     }
     cp_async_4_8(dst, src, esz, ok);
@@ -432,27 +436,29 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   const int64_t kc = k0 + lane * 16;
   if (grow >= a.rows_pad || kc >= kpad) return;
   const bool zero = bs.bad || !bs.mb || k0 >= a.K;
+  const int nslices = a.nslices;
+  const int64_t plane = a.plane;
+  uint8_t *dst = a.panel + panel_tile_base(a, grow, kc);
   double x[16];
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) x[kk] = zero ? 0.0 : scale2(band_value<KIND>(a, tile, w, lane * 16 + kk), -bs.E);
-  const int64_t off = panel_tile_base(a, grow, kc);
-  for (int p = 0; p < a.nslices; ++p) {
+  for (int p = 0; p < nslices; ++p) {
     uint32_t wd[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int kk = 0; kk < 16; ++kk) {
-      // y = 254 x; d = y rounded to the nearest integer (ties to even, like
-      // rint) by adding and removing 1.5 * 2^52, whose low word then holds
-      // d in two's complement; x = y - d.  Four full-rate FP64 adds and
-      // multiplies, no rounding or conversion instructions; the _rn
-      // intrinsics keep the compiler from fusing the steps.
+      // d = 254 x rounded to the nearest integer (ties to even) by one fused
+      // multiply-add with 1.5 * 2^52, whose low word then holds d in two's
+      // complement; x = 254 x - d by a second fused multiply-add (the exact
+      // product, one rounding).  Three full-rate FP64 operations, no
+      // rounding or conversion instructions; the _rn intrinsics keep the
+      // compiler from reassociating the steps.
       constexpr double kRound = 6755399441055744.0;
-      const double y = __dmul_rn(x[kk], 254.0);
-      const double tt = __dadd_rn(y, kRound);
+      const double tt = __fma_rn(x[kk], 254.0, kRound);
       const double d = __dsub_rn(tt, kRound);
-      x[kk] = __dsub_rn(y, d);
+      x[kk] = __fma_rn(x[kk], 254.0, -d);
       wd[kk >> 2] |= ((uint32_t)__double2loint(tt) & 0xFFu) << (8 * (kk & 3));
     }
-    *reinterpret_cast<uint4 *>(a.panel + p * a.plane + off) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    *reinterpret_cast<uint4 *>(dst + p * plane) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
