@@ -584,6 +584,8 @@ static cudaError_t launch_pack_fused(const PackArgs &pa, const PackArgs &pb, int
 // ---------------------------------------------------------------- GEMM ---
 
 enum { KIND_I8 = 0, KIND_BF16 = 1 };
+// K values per FP32-accumulated segment of a BF16x3 tile (4 K blocks).
+constexpr int kBf16SegK = 256;
 
 struct GemmArgs {
   const uint8_t *panelA, *panelB;
@@ -788,8 +790,8 @@ struct GemmCfg<KIND_I8> {
 };
 template <>
 struct GemmCfg<KIND_BF16> {
-  static constexpr int BN = 256, STAGES = 4, KSTEP_BYTES = 32;
-  static constexpr uint32_t IDESC = idesc_bf16(128, 256);
+  static constexpr int BN = 128, STAGES = 6, KSTEP_BYTES = 32;
+  static constexpr uint32_t IDESC = idesc_bf16(128, 128);
 };
 
 template <int KIND>
@@ -833,8 +835,11 @@ __device__ __forceinline__ const GemmArgs &tile_problem(const GemmArgs &a, const
   return g.tab[lo];
 }
 
+// Segments of a tile: Ozaki, one per (diagonal, K segment); BF16x3, one per
+// K segment (FP32 accumulation over at most kBf16SegK K values, the
+// segments summed in FP64).
 __device__ __forceinline__ int seg_count(const GemmArgs &a, int kind) {
-  return kind == KIND_I8 ? a.nslices * a.nkseg : 1;
+  return kind == KIND_I8 ? a.nslices * a.nkseg : a.nkseg;
 }
 // Terms of segment g: (plane of A, plane of B) for term index j, and the K
 // block range.
@@ -852,14 +857,9 @@ __device__ __forceinline__ void seg_term(const GemmArgs &a, int kind, int g, int
   }
 }
 __device__ __forceinline__ void seg_krange(const GemmArgs &a, int kind, int g, int &kb0, int &kb1) {
-  if (kind == KIND_I8) {
-    int ks = g % a.nkseg;
-    kb0 = ks * a.kseg_blocks;
-    kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
-  } else {
-    kb0 = 0;
-    kb1 = a.kblocks;
-  }
+  const int ks = g % a.nkseg;
+  kb0 = ks * a.kseg_blocks;
+  kb1 = min(kb0 + a.kseg_blocks, a.kblocks);
 }
 
 template <int KIND>
@@ -1010,43 +1010,36 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         const bool first = (g == 0), last = (g == nseg - 1);
         const uint32_t tacc = tmem + lane_base + buf * BN;
         const uint32_t tsum = tmem + lane_base + 256;
-        double w = 1.0;
-        if (KIND == KIND_I8) w = P.wdiag[g / P.nkseg];
+        const double w = KIND == KIND_I8 ? P.wdiag[g / P.nkseg] : 1.0;
 #pragma unroll 1
         for (int c = 0; c < BN / 16; ++c) {
           uint32_t dr[16], sr[32];
           tmem_ld16(tacc + 16 * c, dr);
-          if (KIND == KIND_I8 && !first) {
+          if (!first) {
             tmem_ld16(tsum + 32 * c, sr);
             tmem_ld16(tsum + 32 * c + 16, sr + 16);
           }
           tmem_ld_wait();
-          if (KIND == KIND_I8) {
-            double v[16];
+          double v[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const double s0 = first ? 0.0 : __hiloint2double((int)sr[2 * e + 1], (int)sr[2 * e]);
+            const double x = KIND == KIND_I8 ? (double)(int32_t)dr[e] : (double)__uint_as_float(dr[e]);
+            v[e] = fma(x, w, s0);
+          }
+          if (!last) {
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
-              double s0 = first ? 0.0 : __hiloint2double((int)sr[2 * e + 1], (int)sr[2 * e]);
-              v[e] = fma((double)(int32_t)dr[e], w, s0);
+              sr[2 * e] = (uint32_t)__double2loint(v[e]);
+              sr[2 * e + 1] = (uint32_t)__double2hiint(v[e]);
             }
-            if (!last) {
-#pragma unroll
-              for (int e = 0; e < 16; ++e) {
-                sr[2 * e] = (uint32_t)__double2loint(v[e]);
-                sr[2 * e + 1] = (uint32_t)__double2hiint(v[e]);
-              }
-              tmem_st16(tsum + 32 * c, sr);
-              tmem_st16(tsum + 32 * c + 16, sr + 16);
-            } else {
-              store_chunk<double>(P, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
-            }
+            tmem_st16(tsum + 32 * c, sr);
+            tmem_st16(tsum + 32 * c + 16, sr + 16);
           } else {
-            float v[16];
-#pragma unroll
-            for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(dr[e]);
-            store_chunk<float>(P, v, c, n0, row_store, crow, lane, s_offN, s_expN, 0);
+            store_chunk<double>(P, v, c, n0, row_store, crow, lane, s_offN, s_expN, eA);
           }
         }
-        if (KIND == KIND_I8 && !last) tmem_st_wait();
+        if (!last) tmem_st_wait();
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acce[buf]);
@@ -1613,12 +1606,12 @@ void tc_geometry(qs_plan *p) {
     g.nslices = 2;
     g.kblocks = cdiv(Kv, 64);
     g.mtiles = cdiv(Mv, 128);
-    g.ntiles = cdiv(Nv, 256);
+    g.ntiles = cdiv(Nv, 128);
     g.Mp = g.mtiles * 128;
-    g.Np = g.ntiles * 256;
+    g.Np = g.ntiles * 128;
     g.plane_bytes_a = g.mtiles * g.kblocks * 128 * 128;
-    g.plane_bytes_b = g.ntiles * g.kblocks * 256 * 128;
-    g.kseg = (int)g.kblocks;
+    g.plane_bytes_b = g.ntiles * g.kblocks * 128 * 128;
+    g.kseg = (int)std::min<int64_t>(kBf16SegK / 64, g.kblocks);
   }
 }
 
@@ -1750,7 +1743,7 @@ static PackArgs pack_args(const qs_plan *p, int side) {
     a.X = p->Bdata; a.Xbase = p->Bbase; a.TX = p->TB; a.conj = p->conjB;
     a.offR = p->ws.offN[0]; a.offK = p->ws.offK[1];
     a.rows = p->N * g.cols_per_elem_b; a.rows_pad = g.Np;
-    a.tile_rows = p->method == QS_METHOD_BF16X3 ? 256 : 128;
+    a.tile_rows = 128;
     a.cmode = g.cplx_layout == 1 ? 2 : (g.cplx_layout == 2 ? 1 : 0);
     a.rfast = p->b_nfast;
     a.panel = (uint8_t *)p->ws.panelB; a.plane = g.plane_bytes_b;
@@ -1784,8 +1777,8 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.ntiles = (int)g.ntiles;
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
-  a.kseg_blocks = oz ? g.kseg : (int)g.kblocks;
-  a.nkseg = oz ? (int)cdiv(g.kblocks, g.kseg) : 1;
+  a.kseg_blocks = g.kseg;
+  a.nkseg = (int)cdiv(g.kblocks, g.kseg);
   a.expA = p->ws.expA;
   a.expB = p->ws.expB;
   a.C = p->Cdata;
