@@ -76,6 +76,8 @@ struct Workspace {
   int64_t *offM[2] = {nullptr, nullptr};
   int64_t *offN[2] = {nullptr, nullptr};
   int64_t *offK[2] = {nullptr, nullptr};
+  // Ozaki pack: the K maps as int32 (staged in shared memory), or nullptr
+  int32_t *offK32[2] = {nullptr, nullptr};
   // batch labels: [A offsets | B offsets | C offsets], P each, or nullptr
   int64_t *offBatch = nullptr;
   // tensor-core paths: packed operand panels and per-row/col exponents

@@ -2,7 +2,7 @@
 //
 //  * Float64 as an Ozaki-style split: every row of A and every column of B is
 //    scaled by a power of two (its max-magnitude exponent), cut into s signed
-//    base-254 digits (int8 in [-127, 127]), and the slice products are
+//    balanced base-256 digits (int8), and the slice products are
 //    computed exactly on the integer tensor cores (tcgen05.mma kind::i8,
 //    INT32 accumulation in TMEM).
 //    Products of equal weight (p + q = t) share one INT32 accumulator; each
@@ -74,6 +74,9 @@ struct PackArgs {
   // `rows`/`K` above are the real (virtual) extents; offR/offK index the
   // complex elements.
   int cmode;
+  // Real operands (cmode 0): the K offsets as int32 (K entries, padded to a
+  // multiple of 4) when K <= kStageK and every offset fits, else nullptr.
+  const int32_t *offK32;
 };
 
 // Element (r, k) of the real (virtual) matrix the panels hold.
@@ -165,12 +168,17 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
   }
 }
 
-// Ozaki digits of a row (the fused pack below): with E = (frexp exponent of
-// the row's max |x|) + 1, x = v * 2^-E has |x| < 1/2, and
-//   for p = 1..s: y = 254 x; d_p = rint(y); x = y - d_p
-// gives digits |d_p| <= 127 with v ~= 2^E * sum_p d_p 254^-p; the error is
-// the tail 254^-s plus one rounding of 254 x per digit.  Rows with a NaN or
-// Inf get exponent kNonFinite, zero digits, and are listed for the fixup.
+// Ozaki digits of a row (the fused pack below): balanced base-256 digits.
+// With E = (frexp exponent of the row's max |x|) + 1, x = v * 2^-E has
+// |x| < 1/2.  The pack rounds q = x * 127/128 * 2^(8s) once to an integer,
+// so |q| <= 127 * 2^(8s-8), and writes the s bytes of q + sum_i 128 * 256^i
+// (each in 0..255, the sum below 2^(8s)) minus 128 as the digits d_s .. d_1:
+//   v ~= 2^E * 128/127 * sum_p d_p 256^-p,
+// d_1 in [-127, 127] and the others in [-128, 127], all exact int8.  The
+// error is one rounding of q, at most 2^-(8s+1) * 128/127 relative to 2^E
+// (base-254 digits leave (254/256)^s times that).  Rows with a NaN or Inf
+// get exponent kNonFinite, zero digits, and are listed for the fixup.
+constexpr double kDigitScale = 127.0 / 128.0;
 
 // Split-BF16 planes of one 32-row x 64-element block: hi = bf16(x),
 // lo = bf16(x - hi), x in FP32.
@@ -218,12 +226,13 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 }
 
 // Fused Ozaki pack: both passes in one launch, each operand read once from
-// HBM.  A CTA walks bands of kBandRows (virtual) rows of one operand.
-// Phase 1 streams the band's K tiles and reduces every row's max |x| bit
-// pattern in registers (no atomics, nothing to clear per execute); phase 2
-// streams the band again and emits the digit planes.  The grid is two CTAs
-// per SM, so the bands in flight (kBandRows * K * 8 bytes each) stay in L2
-// between the two phases and phase 2 reads them from there.
+// HBM.  A CTA walks a contiguous range of bands of kBandRows (virtual) rows;
+// the ranges are balanced by tile steps.  Phase 1 streams a band's K tiles
+// and reduces every row's max |x| bit pattern in registers (no atomics,
+// nothing to clear per execute); phase 2 streams the band again and emits
+// the digit planes.  Three CTAs per SM keep the bands in flight
+// (kBandRows * K * 8 bytes each) small enough to stay in L2 between the two
+// phases, so phase 2 reads them from there.
 //
 // The tiles move by cp.async into a kPackBufs-deep ring, kPackBufs - 1
 // tiles ahead of the one being processed and across band boundaries, so
@@ -231,12 +240,17 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 // left HBM at 8 % of its bandwidth).  The copies are raw element bytes: a
 // tile slot holds one real value or one complex component (Float32 in its
 // low four bytes), and the virtual matrix (type conversion, conj, the 1e /
-// 1r complex layouts) is formed when a slot is read.
+// 1r complex layouts) is formed when a slot is read.  A real operand's K
+// offsets sit in shared memory as int32 (staged once per operand when
+// K <= kStageK and they fit), so forming a copy's address reads no global
+// memory.
 constexpr int kBandRows = 4, kBandK = 512, kPackBufs = 3;
 constexpr int kPackThreads = 32 * kBandRows;  // a warp per row
-constexpr int kPackCtasPerSm = 4;
+constexpr int kPackCtasPerSm = 3;
 constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 slot per 16, +4 per row: conflict-free
-constexpr size_t kPackSmem = (size_t)kPackBufs * kBandRows * kBandStride * 8;
+constexpr int kStageK = 4608;                          // K offsets staged in shared memory
+constexpr size_t kPackRingBytes = (size_t)kPackBufs * kBandRows * kBandStride * 8;
+constexpr size_t kPackSmem = kPackRingBytes + (size_t)kStageK * sizeof(int32_t);
 
 __device__ __forceinline__ int band_col(int k) { return k + (k >> 4); }
 
@@ -282,51 +296,74 @@ __device__ __forceinline__ void band_seat_rows(const PackArgs &a, int64_t r0, Is
   }
 }
 
+// K offset of index k: from the staged shared-memory table, or from global
+// memory.
+struct SmemKoff {
+  const int32_t *t;
+  __device__ __forceinline__ int64_t operator()(int64_t k) const { return t[k]; }
+};
+struct GlobalKoff {
+  const int64_t *__restrict__ t;
+  __device__ __forceinline__ int64_t operator()(int64_t k) const { return __ldg(t + k); }
+};
+
+// The copies of a real operand's K tile [k0, k0 + kBandK) (element size ESZ).
+template <int ESZ, class Koff>
+__device__ __forceinline__ void band_issue_real(const PackArgs &a, int64_t k0, uint32_t tile, const IssueRows &ir,
+                                                Koff koff) {
+  const int tid = threadIdx.x;
+  const char *X = static_cast<const char *>(a.X);
+  const int64_t K = a.K;
+  if (a.rfast) {
+    const int rr = tid % kBandRows, kb = tid / kBandRows;
+    const int64_t ro = ir.ro[0];
+#pragma unroll
+    for (int i = 0; i < kBandK / (kPackThreads / kBandRows); ++i) {
+      const int kk = kb + (kPackThreads / kBandRows) * i;
+      const int64_t k = k0 + kk;
+      const bool ok = ro != INT64_MIN && k < K;
+      const char *src = ok ? X + (ro + koff(k)) * ESZ : X;
+      cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < kBandK / kPackThreads; ++h) {
+      const int kk = tid + kPackThreads * h;
+      const int64_t k = k0 + kk;
+      const bool kok = k < K;
+      const int64_t ko = kok ? koff(k) : 0;
+#pragma unroll
+      for (int rr = 0; rr < kBandRows; ++rr) {
+        const bool ok = kok && ir.ro[rr] != INT64_MIN;
+        const char *src = ok ? X + (ir.ro[rr] + ko) * ESZ : X;
+        cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
+      }
+    }
+  }
+}
+
 // Issue the copies of K tile [k0, k0 + kBandK) of virtual rows
 // [r0, r0 + kBandRows) into `tile` (slot (row, k) at row * kBandStride +
 // band_col(k)), zero-filled outside the operand, coalesced along X's
-// unit-stride axis.  Real operands: slot = element.  General path: 1r
-// (cmode 2, K doubled): slots 2j, 2j+1 = re, im of complex K index j; 1e
-// (cmode 1, rows and K doubled): complex row i goes to even row 2i as in 1r
-// and odd rows are formed from it on read; a real operand in a complex
-// layout gets zero imaginary slots.
+// unit-stride axis.  Real operands: slot = element, K offsets from `skoff`
+// (the staged table) when it is not null.  General path: 1r (cmode 2, K
+// doubled): slots 2j, 2j+1 = re, im of complex K index j; 1e (cmode 1, rows
+// and K doubled): complex row i goes to even row 2i as in 1r and odd rows are
+// formed from it on read; a real operand in a complex layout gets zero
+// imaginary slots.
 template <int KIND>
 __device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_t k0, uint32_t tile,
-                                           const IssueRows &ir) {
+                                           const IssueRows &ir, const int32_t *skoff) {
+  if constexpr (KIND != kPackAny) {
+    constexpr int ESZ = KIND == kPackF64 ? 8 : 4;
+    if (skoff) band_issue_real<ESZ>(a, k0, tile, ir, SmemKoff{skoff});
+    else band_issue_real<ESZ>(a, k0, tile, ir, GlobalKoff{a.offK});
+    return;
+  }
   const int tid = threadIdx.x;
   const char *X = static_cast<const char *>(a.X);
   const int64_t K = a.K;
   const int64_t *__restrict__ offK = a.offK;
-  if constexpr (KIND != kPackAny) {
-    constexpr int ESZ = KIND == kPackF64 ? 8 : 4;
-    if (a.rfast) {
-      const int rr = tid % kBandRows, kb = tid / kBandRows;
-      const int64_t ro = ir.ro[0];
-#pragma unroll
-      for (int i = 0; i < kBandK / (kPackThreads / kBandRows); ++i) {
-        const int kk = kb + (kPackThreads / kBandRows) * i;
-        const int64_t k = k0 + kk;
-        const bool ok = ro != INT64_MIN && k < K;
-        const char *src = ok ? X + (ro + __ldg(offK + k)) * ESZ : X;
-        cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
-      }
-    } else {
-#pragma unroll
-      for (int h = 0; h < kBandK / kPackThreads; ++h) {
-        const int kk = tid + kPackThreads * h;
-        const int64_t k = k0 + kk;
-        const bool kok = k < K;
-        const int64_t ko = kok ? __ldg(offK + k) : 0;
-#pragma unroll
-        for (int rr = 0; rr < kBandRows; ++rr) {
-          const bool ok = kok && ir.ro[rr] != INT64_MIN;
-          const char *src = ok ? X + (ir.ro[rr] + ko) * ESZ : X;
-          cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
-        }
-      }
-    }
-    return;
-  }
   const bool cx = a.TX == QS_C32 || a.TX == QS_C64;
   const int esz = (a.TX == QS_F64 || a.TX == QS_C64) ? 8 : 4;
   const int cmode = a.cmode;
@@ -389,6 +426,8 @@ struct BandState {
   unsigned long long mb;  // running max |x| bit pattern of this warp's row
   int E;
   bool bad;
+  bool wide;  // 2^(8s - E) is outside the normal range: scale in two steps
+  double f;   // the digit scale 127/128 * 2^(8s - E) (wide: 127/128 * 2^(8s))
 };
 
 // Process tile `t` (phase 1: t < nk1; phase 2 otherwise) of the band at
@@ -400,6 +439,7 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
                                              BandState &bs) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t grow = r0 + w;
+  const int s = a.nslices;
   if (t < nk1) {
     if (t == 0) bs.mb = 0;
 #pragma unroll
@@ -418,11 +458,16 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
       // zero digits and a place on the fixup list.
       bs.E = 0;
       bs.bad = bs.mb >= 0x7FF0000000000000ull;
+      bs.wide = false;
+      bs.f = 0.0;
       if (bs.bad) {
         bs.E = kNonFinite;
       } else if (bs.mb) {
         frexp(__longlong_as_double((long long)bs.mb), &bs.E);
         bs.E += 1;
+        const int sh = 8 * s - bs.E;
+        bs.wide = sh < -1000 || sh > 1000;
+        bs.f = kDigitScale * __longlong_as_double((long long)((bs.wide ? 8 * s : sh) + 1023) << 52);
       }
       if (grow < a.rows_pad && lane == 0) {
         a.exp_out[grow] = bs.E;
@@ -436,83 +481,138 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   const int64_t kc = k0 + lane * 16;
   if (grow >= a.rows_pad || kc >= kpad) return;
   const bool zero = bs.bad || !bs.mb || k0 >= a.K;
-  const int nslices = a.nslices;
   const int64_t plane = a.plane;
   uint8_t *dst = a.panel + panel_tile_base(a, grow, kc);
-  double x[16];
+  // Digits (the balanced base-256 expansion described above): q = the row's
+  // value scaled by f and rounded once to an integer, |q| <= 127 * 2^(8s-8);
+  // the bytes of q + 0x80..80 (s bytes) are the digits + 128, low digit
+  // first.
+  const unsigned long long bias = 0x8080808080808080ull >> (64 - 8 * s);
+  uint32_t lo[16], hi[16];
 #pragma unroll
-  for (int kk = 0; kk < 16; ++kk) x[kk] = zero ? 0.0 : scale2(band_value<KIND>(a, tile, w, lane * 16 + kk), -bs.E);
-  for (int p = 0; p < nslices; ++p) {
-    uint32_t wd[4] = {0, 0, 0, 0};
+  for (int kk = 0; kk < 16; ++kk) {
+    double y = 0.0;
+    if (!zero) {
+      const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
+      y = bs.wide ? scale2(v, -bs.E) * bs.f : v * bs.f;
+    }
+    const unsigned long long u = (unsigned long long)__double2ll_rn(y) + bias;
+    lo[kk] = (uint32_t)u;
+    hi[kk] = (uint32_t)(u >> 32);
+  }
+  for (int p = 0; p < s; ++p) {
+    // plane p holds digit p + 1 (weight 256^-(p+1)): byte s - 1 - p of q + bias
+    const int bi = s - 1 - p;
+    const uint32_t sel = 0x11u * (uint32_t)(bi & 3) + 0x40u;  // byte bi of x, byte bi of y
+    uint32_t wd[4];
+    if (bi >= 4) {
 #pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      // d = 254 x rounded to the nearest integer (ties to even) by one fused
-      // multiply-add with 1.5 * 2^52, whose low word then holds d in two's
-      // complement; x = 254 x - d by a second fused multiply-add (the exact
-      // product, one rounding).  Three full-rate FP64 operations, no
-      // rounding or conversion instructions; the _rn intrinsics keep the
-      // compiler from reassociating the steps.
-      constexpr double kRound = 6755399441055744.0;
-      const double tt = __fma_rn(x[kk], 254.0, kRound);
-      const double d = __dsub_rn(tt, kRound);
-      x[kk] = __fma_rn(x[kk], 254.0, -d);
-      wd[kk >> 2] |= ((uint32_t)__double2loint(tt) & 0xFFu) << (8 * (kk & 3));
+      for (int j = 0; j < 4; ++j)
+        wd[j] = __byte_perm(__byte_perm(hi[4 * j], hi[4 * j + 1], sel), __byte_perm(hi[4 * j + 2], hi[4 * j + 3], sel),
+                            0x5410) ^ 0x80808080u;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        wd[j] = __byte_perm(__byte_perm(lo[4 * j], lo[4 * j + 1], sel), __byte_perm(lo[4 * j + 2], lo[4 * j + 3], sel),
+                            0x5410) ^ 0x80808080u;
     }
     *reinterpret_cast<uint4 *>(dst + p * plane) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
-// A walk over this CTA's bands, one tile step at a time: band index
-// b = blockIdx.x + n * gridDim.x, steps 0 .. nk1 + nk2 - 1 per band
-// (nk1 tiles of phase 1, nk2 of phase 2; phase-2 tiles past K load nothing).
-// `Bands` maps a band index to its PackArgs and first row.
+// Steps of one band: nk1 tiles of phase 1, nk2 of phase 2.
+__host__ __device__ inline int band_nk1(int64_t K) { return (int)((K + kBandK - 1) / kBandK); }
+__host__ __device__ inline int band_nk2(int kblocks) { return (int)(((int64_t)kblocks * kKBytes + kBandK - 1) / kBandK); }
+
+// A walk over this CTA's bands [b, end), one tile step at a time: steps
+// 0 .. nk1 + nk2 - 1 per band (phase-2 tiles past K load nothing).  `Bands`
+// maps band indices to jobs (an operand of a problem: its PackArgs and its
+// first band); the cursor follows the job index as it moves.
 template <class Bands>
 struct BandCursor {
-  int64_t b;
+  int64_t b, end;
   int t;
+  int job;
+  int64_t jfirst, jend;
   const PackArgs *a;
   int64_t r0;
   int nk1, nk2;
-  __device__ __forceinline__ void seat(const Bands &bands) {
-    if (b < bands.count()) {
-      a = bands.args(b, r0);
-      nk1 = (int)((a->K + kBandK - 1) / kBandK);
-      nk2 = (int)(((int64_t)a->kblocks * kKBytes + kBandK - 1) / kBandK);
+  __device__ __forceinline__ void start(const Bands &bands, int64_t b0, int64_t b1) {
+    b = b0;
+    end = b1;
+    t = 0;
+    if (b < end) {
+      job = bands.find(b);
+      enter(bands);
     }
   }
-  __device__ __forceinline__ bool valid(const Bands &bands) const { return b < bands.count(); }
+  __device__ __forceinline__ void enter(const Bands &bands) {
+    a = bands.args(job);
+    jfirst = bands.first(job);
+    jend = bands.last(job);
+    nk1 = band_nk1(a->K);
+    nk2 = band_nk2(a->kblocks);
+    r0 = (b - jfirst) * kBandRows;
+  }
+  __device__ __forceinline__ bool valid() const { return b < end; }
   // Advances one step; true when it moved to a new band.
   __device__ __forceinline__ bool next(const Bands &bands) {
     if (++t < nk1 + nk2) return false;
     t = 0;
-    b += gridDim.x;
-    seat(bands);
+    if (++b < end) {
+      if (b >= jend) {
+        do ++job;
+        while (bands.last(job) <= b);
+        enter(bands);
+      } else {
+        r0 += kBandRows;
+      }
+    }
     return true;
   }
 };
 
 template <int KIND, class Bands>
-__device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring) {
+__device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring, int32_t *skoff) {
   const uint32_t ring_u32 = smem_u32(ring);
   constexpr uint32_t kTileBytes = kBandRows * kBandStride * 8;
-  BandCursor<Bands> in{(int64_t)blockIdx.x, 0, nullptr, 0, 0, 0}, out = in;
-  in.seat(bands);
-  out.seat(bands);
+  int64_t b0, b1;
+  bands.range(blockIdx.x, gridDim.x, b0, b1);
+  BandCursor<Bands> in, out;
+  in.start(bands, b0, b1);
+  out.start(bands, b0, b1);
   IssueRows ir;
-  if (in.valid(bands)) band_seat_rows<KIND>(*in.a, in.r0, ir);
+  if (in.valid()) band_seat_rows<KIND>(*in.a, in.r0, ir);
+  const PackArgs *staged = nullptr;  // the operand whose K offsets are in skoff
   uint32_t issued = 0, done = 0;
   auto issue = [&]() {
-    if (in.valid(bands)) {
+    if (in.valid()) {
+      const int32_t *ko = nullptr;
+      if constexpr (KIND != kPackAny) {
+        if (in.a->offK32) {
+          if (in.a != staged) {
+            // Uniform over the CTA (one cursor): no thread reads the old
+            // table past the first barrier.
+            __syncthreads();
+            const int n4 = (int)((in.a->K + 3) >> 2);
+            const int4 *src = reinterpret_cast<const int4 *>(in.a->offK32);
+            for (int i = threadIdx.x; i < n4; i += kPackThreads) reinterpret_cast<int4 *>(skoff)[i] = __ldg(src + i);
+            __syncthreads();
+            staged = in.a;
+          }
+          ko = skoff;
+        }
+      }
       const int64_t k0 = (int64_t)(in.t < in.nk1 ? in.t : in.t - in.nk1) * kBandK;
-      if (k0 < in.a->K) band_issue<KIND>(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes, ir);
-      if (in.next(bands) && in.valid(bands)) band_seat_rows<KIND>(*in.a, in.r0, ir);
+      if (k0 < in.a->K) band_issue<KIND>(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes, ir, ko);
+      if (in.next(bands) && in.valid()) band_seat_rows<KIND>(*in.a, in.r0, ir);
     }
     cp_async_commit();
     ++issued;
   };
   for (int q = 0; q < kPackBufs - 1; ++q) issue();
-  BandState bs{0, 0, false};
-  while (out.valid(bands)) {
+  BandState bs{0, 0, false, false, 0.0};
+  while (out.valid()) {
     cp_async_wait<kPackBufs - 2>();  // this step's tile has landed (for this thread)
     __syncthreads();                 // ... for every thread; the oldest buffer is free again
     issue();
@@ -524,18 +624,34 @@ __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring) {
   cp_async_wait<0>();
 }
 
+// The band range [b0, b1) of CTA c of G: the bands whose first step lies in
+// [c T / G, (c + 1) T / G), T the total steps, for jobs whose bands take
+// `steps[j]` steps each.  Host and device share it.
+__host__ __device__ inline int64_t band_at_step(int64_t P, int njobs, const int64_t *nb, const int64_t *steps) {
+  int64_t b = 0;
+  for (int j = 0; j < njobs; ++j) {
+    const int64_t span = nb[j] * steps[j];
+    if (P <= span) return b + (P + steps[j] - 1) / steps[j];
+    P -= span;
+    b += nb[j];
+  }
+  return b;
+}
+
 // Both operands of one plan: bands [0, nbA) of A, then [0, nbB) of B.
 struct PairBands {
   const PackArgs *pa, *pb;
   int64_t nbA, nbB;
-  __device__ __forceinline__ int64_t count() const { return nbA + nbB; }
-  __device__ __forceinline__ const PackArgs *args(int64_t b, int64_t &r0) const {
-    if (b < nbA) {
-      r0 = b * kBandRows;
-      return pa;
-    }
-    r0 = (b - nbA) * kBandRows;
-    return pb;
+  __device__ __forceinline__ int find(int64_t b) const { return b < nbA ? 0 : 1; }
+  __device__ __forceinline__ const PackArgs *args(int j) const { return j == 0 ? pa : pb; }
+  __device__ __forceinline__ int64_t first(int j) const { return j == 0 ? 0 : nbA; }
+  __device__ __forceinline__ int64_t last(int j) const { return j == 0 ? nbA : nbA + nbB; }
+  __device__ __forceinline__ void range(int c, int G, int64_t &b0, int64_t &b1) const {
+    const int64_t nb[2] = {nbA, nbB};
+    const int64_t st[2] = {band_nk1(pa->K) + band_nk2(pa->kblocks), band_nk1(pb->K) + band_nk2(pb->kblocks)};
+    const int64_t T = nbA * st[0] + nbB * st[1];
+    b0 = band_at_step(T * c / G, 2, nb, st);
+    b1 = band_at_step(T * (c + 1) / G, 2, nb, st);
   }
 };
 
@@ -544,7 +660,8 @@ __global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
     oz_pack_fused_kernel(const __grid_constant__ PackArgs pa, const __grid_constant__ PackArgs pb, int64_t nbA,
                          int64_t nbB) {
   extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk<KIND>(PairBands{&pa, &pb, nbA, nbB}, pack_ring);
+  oz_pack_walk<KIND>(PairBands{&pa, &pb, nbA, nbB}, pack_ring,
+                     reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(pack_ring) + kPackRingBytes));
 }
 
 // The kind both operands share, else the general path.
@@ -606,7 +723,7 @@ struct GemmArgs {
   int cplx;  // 0 real; 1 = 1m: real rows 2i / 2i+1 are Re / Im of complex
              // row i; 2 = planar: real columns 2n / 2n+1 are Re / Im of n
   int *status;
-  double wdiag[16];  // weight of diagonal t (Ozaki): 254^-(t+2)
+  double wdiag[16];  // weight of diagonal t (Ozaki): (128/127)^2 256^-(t+2)
   uint64_t wait_ns;  // bound of every barrier wait (qs_plan_set_wait_limit)
   int hold_loads;    // failure-detection test: the producers issue no copies
   int band_m;        // tile raster: m-tiles per band (Ozaki kernels)
@@ -1548,7 +1665,7 @@ int tc_auto_method(const qs_plan *p) {
 static bool oz_fixed_slices(int s) { return s == 4 || s == 6 || s == 7; }
 
 static int default_slices(int64_t K, bool cplx, bool dbl) {
-  // The relative error of s base-254 digits is about 254^-s times
+  // The relative error of s base-256 digits is about 256^-s times
   // (row max / row rms of A + column max / column rms of B): ~1e-14 for
   // s = 6 on uniform inputs at K = 2304 (max/rms = sqrt 3), but up to ~1e-13
   // for Gaussian rows of a few thousand elements (max/rms ~ 4), which the
@@ -1598,8 +1715,9 @@ void tc_geometry(qs_plan *p) {
     g.Np = g.ntiles * 128;
     g.plane_bytes_a = mt_alloc * g.kblocks * 128 * 128;
     g.plane_bytes_b = g.ntiles * g.kblocks * 128 * 128;
-    // INT32-exact segment: (terms) * kblocks * 128 * 127^2 < 2^31.
-    int64_t maxkb = (int64_t)(2147483647ll / ((int64_t)g.nslices * 128 * 127 * 127));
+    // INT32-exact segment: (terms) * kblocks * 128 * 128^2 < 2^31 (digits
+    // in [-128, 127]).
+    int64_t maxkb = (int64_t)(2147483647ll / ((int64_t)g.nslices * 128 * 128 * 128));
     if (maxkb < 1) maxkb = 1;
     g.kseg = (int)std::min<int64_t>(maxkb, g.kblocks);
   } else {
@@ -1660,6 +1778,30 @@ static bool make_pair_maps(qs_plan *p) {
   return true;
 }
 
+// The int32 copy of a real operand's K map for the fused pack's staged
+// table: only when the operand is real (no complex layout), K <= kStageK and
+// every offset fits in int32; else the pack reads the int64 map.
+static int upload_koff32(qs_plan *p, int side) {
+  const TensorCoreGeom &g = p->tc;
+  const int T = side == 0 ? p->TA : p->TB;
+  if (g.cplx_layout != 0 || is_complex(T) || p->K <= 0 || p->K > kStageK) return QS_OK;
+  int64_t lo, hi;
+  p->kg.offset_range(side, lo, hi);
+  if (lo < INT32_MIN || hi > INT32_MAX) return QS_OK;
+  std::vector<int64_t> o((size_t)p->K);
+  p->kg.fill_offsets(side, 0, p->K, o.data());
+  std::vector<int32_t> h((size_t)((p->K + 3) & ~int64_t(3)), 0);
+  for (int64_t k = 0; k < p->K; ++k) h[(size_t)k] = (int32_t)o[(size_t)k];
+  void *q;
+  int rc = tc_alloc(p, &q, h.size() * sizeof(int32_t));
+  if (rc) return rc;
+  if (reinterpret_cast<uintptr_t>(q) & 15) return QS_OK;  // a caller allocator's odd block: int64 map
+  if (setup_upload(q, h.data(), h.size() * sizeof(int32_t)) != cudaSuccess)
+    return fail(QS_ECUDA, "cudaMemcpyAsync (int32 K offsets)");
+  p->ws.offK32[side] = (int32_t *)q;
+  return QS_OK;
+}
+
 int tc_prepare(qs_plan *p) {
   tc_geometry(p);
   const TensorCoreGeom &g = p->tc;
@@ -1669,6 +1811,9 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelA = q;
   if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_b * g.nslices))) return rc;
   p->ws.panelB = q;
+  if (p->method == QS_METHOD_OZAKI_I8)
+    for (int side = 0; side < 2; ++side)
+      if ((rc = upload_koff32(p, side))) return rc;
   if (p->method == QS_METHOD_OZAKI_I8 && oz_fixed_slices(g.nslices) &&
       !(p->opts.flags & (QS_PLAN_OZ_SINGLE_SM | QS_PLAN_PER_PRODUCT_GEMM)))
     p->oz_pair_maps = make_pair_maps(p) ? 1 : 0;  // else the one-SM kernel runs
@@ -1752,6 +1897,7 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   a.K = p->K * g.kmul;
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
+  a.offK32 = p->ws.offK32[side];
   if (p->method == QS_METHOD_OZAKI_I8) {
     int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
     int32_t *counters = lists + g.Mp + g.Np;
@@ -1798,7 +1944,10 @@ static GemmArgs make_gemm_args(const qs_plan *p, const double *alpha, const doub
   a.beta = cv(beta[0]);
   a.beta_case = beta_case;
   a.status = p->ws.status;
-  for (int t = 0; t < 16; ++t) a.wdiag[t] = std::pow(254.0, -(double)(t + 2));
+  // Diagonal t holds products of digits p + q = t + 2 (weight 256^-(t+2)),
+  // times (128/127)^2 for the two operands' digit scale.
+  const double undo = (128.0 / 127.0) * (128.0 / 127.0);
+  for (int t = 0; t < 16; ++t) a.wdiag[t] = std::ldexp(undo, -8 * (t + 2));
   a.wait_ns = p->wait_ns;
   a.hold_loads = p->hold_loads;
   a.band_m = kOzBandM;
@@ -1987,22 +2136,30 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
     jobs[j >> 1].counters[j & 1] = 0;
 }
 
-// The fused pack over every band of every (problem, side) job.
+// The fused pack over every band of every (problem, side) job; CTA c walks
+// bands [band_start[c], band_start[c + 1]) (balanced by steps on the host).
 struct GroupBands {
   const PackJob *jobs;
+  const int *band_start;
   int njobs, nbands;
-  __device__ __forceinline__ int64_t count() const { return nbands; }
-  __device__ __forceinline__ const PackArgs *args(int64_t b, int64_t &r0) const {
-    const PackJob &j = jobs[pack_job(jobs, njobs, (int)b)];
-    r0 = (b - j.block_start) * kBandRows;
-    return &j.pa;
+  __device__ __forceinline__ int find(int64_t b) const { return pack_job(jobs, njobs, (int)b); }
+  __device__ __forceinline__ const PackArgs *args(int j) const { return &jobs[j].pa; }
+  __device__ __forceinline__ int64_t first(int j) const { return jobs[j].block_start; }
+  __device__ __forceinline__ int64_t last(int j) const {
+    return j + 1 < njobs ? jobs[j + 1].block_start : nbands;
+  }
+  __device__ __forceinline__ void range(int c, int, int64_t &b0, int64_t &b1) const {
+    b0 = band_start[c];
+    b1 = band_start[c + 1];
   }
 };
 
 template <int KIND>
-__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm) oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
+__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
+    oz_pack_fused_grouped(const PackJob *jobs, const int *band_start, int njobs, int nbands) {
   extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk<KIND>(GroupBands{jobs, njobs, nbands}, pack_ring);
+  oz_pack_walk<KIND>(GroupBands{jobs, band_start, njobs, nbands}, pack_ring,
+                     reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(pack_ring) + kPackRingBytes));
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
@@ -2076,6 +2233,21 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
       if (pack_kind_of(j.pa) != g.pack_kind) g.pack_kind = kPackAny;
   }
   g.tiles = tiles.back();
+  // Fused pack: each CTA's contiguous band range, balanced by tile steps.
+  std::vector<int> bstart;
+  if (oz && blocks > 0) {
+    g.pack_grid = (int)std::min<int64_t>(blocks, (int64_t)kPackCtasPerSm * num_sms());
+    std::vector<int64_t> nb(jobs.size()), st(jobs.size());
+    int64_t T = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      nb[j] = jobs[j].gx;
+      st[j] = band_nk1(jobs[j].pa.K) + band_nk2(jobs[j].pa.kblocks);
+      T += nb[j] * st[j];
+    }
+    bstart.resize((size_t)g.pack_grid + 1);
+    for (int c = 0; c <= g.pack_grid; ++c)
+      bstart[(size_t)c] = (int)band_at_step(T * c / g.pack_grid, (int)jobs.size(), nb.data(), st.data());
+  }
   size_t off = 0;
   g.off_pack = off;
   off = align_up(off + jobs.size() * sizeof(PackJob), 64);
@@ -2087,6 +2259,8 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   off = align_up(off + zero.size() * sizeof(ZeroJob), 64);
   g.off_fix = off;
   off = align_up(off + fix.size() * sizeof(FixupJob), 64);
+  g.off_bstart = off;
+  off = align_up(off + bstart.size() * sizeof(int), 64);
   g.image.assign(off, 0);
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes) std::memcpy(g.image.data() + at, src, bytes);
@@ -2096,6 +2270,7 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   put(g.off_tiles, tiles.data(), tiles.size() * sizeof(int));
   put(g.off_zero, zero.data(), zero.size() * sizeof(ZeroJob));
   put(g.off_fix, fix.data(), fix.size() * sizeof(FixupJob));
+  put(g.off_bstart, bstart.data(), bstart.size() * sizeof(int));
   return QS_OK;
 }
 
@@ -2140,19 +2315,22 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const int pgrid = std::min(n, 4 * num_sms());
     oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
     static std::atomic<int> done[3];
-    const int pgrid2 = std::min(g.pack_blocks, kPackCtasPerSm * num_sms());
-    switch (g.pack_kind) {
+    const int pgrid2 = g.pack_grid;
+    const int *bstart = (const int *)(d + g.off_bstart);
+    switch (pgrid2 > 0 ? g.pack_kind : -1) {
+      case -1:
+        break;
       case kPackF64:
         pack_smem_attr(oz_pack_fused_grouped<kPackF64>, done[0]);
-        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
         break;
       case kPackF32:
         pack_smem_attr(oz_pack_fused_grouped<kPackF32>, done[1]);
-        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
         break;
       default:
         pack_smem_attr(oz_pack_fused_grouped<kPackAny>, done[2]);
-        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
         break;
     }
     if (g.cls == TC_CLASS_OZ4)
