@@ -524,73 +524,89 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
 __host__ __device__ inline int band_nk1(int64_t K) { return (int)((K + kBandK - 1) / kBandK); }
 __host__ __device__ inline int band_nk2(int kblocks) { return (int)(((int64_t)kblocks * kKBytes + kBandK - 1) / kBandK); }
 
-// A walk over this CTA's bands [b, end), one tile step at a time: steps
-// 0 .. nk1 + nk2 - 1 per band (phase-2 tiles past K load nothing).  `Bands`
-// maps band indices to jobs (an operand of a problem: its PackArgs and its
-// first band); the cursor follows the job index as it moves.
+// A walk over this CTA's bands b = blockIdx.x + n * gridDim.x (neighbouring
+// bands in neighbouring CTAs, so the rows of an M-fast operand that share a
+// DRAM burst are read at about the same time), one tile step at a time:
+// steps 0 .. nk1 + nk2 - 1 per band (phase-2 tiles past K load nothing).
+// `Bands` maps band indices to jobs (one operand of one problem: its
+// PackArgs and first band); the cursor follows the job index forward.  Each
+// band's PackArgs is copied into one of the cursor's two shared-memory
+// slots, so the loops read shared memory rather than the parameter or job
+// table through a runtime-selected pointer.
 template <class Bands>
 struct BandCursor {
-  int64_t b, end;
+  int64_t b;
   int t;
   int job;
   int64_t jfirst, jend;
+  PackArgs *slots;  // two shared-memory slots, alternating per band
+  int par;
   const PackArgs *a;
   int64_t r0;
   int nk1, nk2;
-  __device__ __forceinline__ void start(const Bands &bands, int64_t b0, int64_t b1) {
-    b = b0;
-    end = b1;
+  __device__ __forceinline__ void start(const Bands &bands, PackArgs *s2) {
+    b = blockIdx.x;
     t = 0;
-    if (b < end) {
+    slots = s2;
+    par = 0;
+    if (b < bands.count()) {
       job = bands.find(b);
       enter(bands);
     }
   }
+  // Copies the job's PackArgs (every thread of the CTA calls it; the copy is
+  // read after the next __syncthreads).
   __device__ __forceinline__ void enter(const Bands &bands) {
-    a = bands.args(job);
+    const PackArgs *src = bands.args(job);
+    par ^= 1;
+    uint64_t *d = reinterpret_cast<uint64_t *>(&slots[par]);
+    const uint64_t *s = reinterpret_cast<const uint64_t *>(src);
+    for (int i = threadIdx.x; i < (int)(sizeof(PackArgs) / 8); i += kPackThreads) d[i] = s[i];
+    a = &slots[par];
     jfirst = bands.first(job);
     jend = bands.last(job);
-    nk1 = band_nk1(a->K);
-    nk2 = band_nk2(a->kblocks);
+    nk1 = band_nk1(src->K);
+    nk2 = band_nk2(src->kblocks);
     r0 = (b - jfirst) * kBandRows;
   }
-  __device__ __forceinline__ bool valid() const { return b < end; }
+  __device__ __forceinline__ const PackArgs *source(const Bands &bands) const { return bands.args(job); }
+  __device__ __forceinline__ bool valid(const Bands &bands) const { return b < bands.count(); }
   // Advances one step; true when it moved to a new band.
   __device__ __forceinline__ bool next(const Bands &bands) {
     if (++t < nk1 + nk2) return false;
     t = 0;
-    if (++b < end) {
+    b += gridDim.x;
+    if (b < bands.count()) {
       if (b >= jend) {
         do ++job;
         while (bands.last(job) <= b);
-        enter(bands);
-      } else {
-        r0 += kBandRows;
       }
+      enter(bands);
     }
     return true;
   }
 };
+static_assert(sizeof(PackArgs) % 8 == 0, "PackArgs copies as 8-byte words");
 
 template <int KIND, class Bands>
 __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring, int32_t *skoff) {
+  __shared__ PackArgs s_args[4];  // [issue cursor: 2][process cursor: 2]
   const uint32_t ring_u32 = smem_u32(ring);
   constexpr uint32_t kTileBytes = kBandRows * kBandStride * 8;
-  int64_t b0, b1;
-  bands.range(blockIdx.x, gridDim.x, b0, b1);
   BandCursor<Bands> in, out;
-  in.start(bands, b0, b1);
-  out.start(bands, b0, b1);
+  in.start(bands, s_args);
+  out.start(bands, s_args + 2);
   IssueRows ir;
-  if (in.valid()) band_seat_rows<KIND>(*in.a, in.r0, ir);
-  const PackArgs *staged = nullptr;  // the operand whose K offsets are in skoff
+  if (in.valid(bands)) band_seat_rows<KIND>(*in.source(bands), in.r0, ir);
+  __syncthreads();  // the first slots are filled
+  int staged = -1;  // the job whose K offsets are in skoff
   uint32_t issued = 0, done = 0;
   auto issue = [&]() {
-    if (in.valid()) {
+    if (in.valid(bands)) {
       const int32_t *ko = nullptr;
       if constexpr (KIND != kPackAny) {
         if (in.a->offK32) {
-          if (in.a != staged) {
+          if (in.job != staged) {
             // Uniform over the CTA (one cursor): no thread reads the old
             // table past the first barrier.
             __syncthreads();
@@ -598,21 +614,24 @@ __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring, i
             const int4 *src = reinterpret_cast<const int4 *>(in.a->offK32);
             for (int i = threadIdx.x; i < n4; i += kPackThreads) reinterpret_cast<int4 *>(skoff)[i] = __ldg(src + i);
             __syncthreads();
-            staged = in.a;
+            staged = in.job;
           }
           ko = skoff;
         }
       }
       const int64_t k0 = (int64_t)(in.t < in.nk1 ? in.t : in.t - in.nk1) * kBandK;
       if (k0 < in.a->K) band_issue<KIND>(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes, ir, ko);
-      if (in.next(bands) && in.valid()) band_seat_rows<KIND>(*in.a, in.r0, ir);
+      if (in.next(bands) && in.valid(bands)) band_seat_rows<KIND>(*in.source(bands), in.r0, ir);
     }
     cp_async_commit();
     ++issued;
   };
-  for (int q = 0; q < kPackBufs - 1; ++q) issue();
+  for (int q = 0; q < kPackBufs - 1; ++q) {
+    issue();
+    __syncthreads();  // a slot the issue filled is read by the next one
+  }
   BandState bs{0, 0, false, false, 0.0};
-  while (out.valid()) {
+  while (out.valid(bands)) {
     cp_async_wait<kPackBufs - 2>();  // this step's tile has landed (for this thread)
     __syncthreads();                 // ... for every thread; the oldest buffer is free again
     issue();
@@ -624,35 +643,15 @@ __device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring, i
   cp_async_wait<0>();
 }
 
-// The band range [b0, b1) of CTA c of G: the bands whose first step lies in
-// [c T / G, (c + 1) T / G), T the total steps, for jobs whose bands take
-// `steps[j]` steps each.  Host and device share it.
-__host__ __device__ inline int64_t band_at_step(int64_t P, int njobs, const int64_t *nb, const int64_t *steps) {
-  int64_t b = 0;
-  for (int j = 0; j < njobs; ++j) {
-    const int64_t span = nb[j] * steps[j];
-    if (P <= span) return b + (P + steps[j] - 1) / steps[j];
-    P -= span;
-    b += nb[j];
-  }
-  return b;
-}
-
 // Both operands of one plan: bands [0, nbA) of A, then [0, nbB) of B.
 struct PairBands {
   const PackArgs *pa, *pb;
   int64_t nbA, nbB;
+  __device__ __forceinline__ int64_t count() const { return nbA + nbB; }
   __device__ __forceinline__ int find(int64_t b) const { return b < nbA ? 0 : 1; }
   __device__ __forceinline__ const PackArgs *args(int j) const { return j == 0 ? pa : pb; }
   __device__ __forceinline__ int64_t first(int j) const { return j == 0 ? 0 : nbA; }
   __device__ __forceinline__ int64_t last(int j) const { return j == 0 ? nbA : nbA + nbB; }
-  __device__ __forceinline__ void range(int c, int G, int64_t &b0, int64_t &b1) const {
-    const int64_t nb[2] = {nbA, nbB};
-    const int64_t st[2] = {band_nk1(pa->K) + band_nk2(pa->kblocks), band_nk1(pb->K) + band_nk2(pb->kblocks)};
-    const int64_t T = nbA * st[0] + nbB * st[1];
-    b0 = band_at_step(T * c / G, 2, nb, st);
-    b1 = band_at_step(T * (c + 1) / G, 2, nb, st);
-  }
 };
 
 template <int KIND>
@@ -2136,29 +2135,24 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
     jobs[j >> 1].counters[j & 1] = 0;
 }
 
-// The fused pack over every band of every (problem, side) job; CTA c walks
-// bands [band_start[c], band_start[c + 1]) (balanced by steps on the host).
+// The fused pack over every band of every (problem, side) job.
 struct GroupBands {
   const PackJob *jobs;
-  const int *band_start;
   int njobs, nbands;
+  __device__ __forceinline__ int64_t count() const { return nbands; }
   __device__ __forceinline__ int find(int64_t b) const { return pack_job(jobs, njobs, (int)b); }
   __device__ __forceinline__ const PackArgs *args(int j) const { return &jobs[j].pa; }
   __device__ __forceinline__ int64_t first(int j) const { return jobs[j].block_start; }
   __device__ __forceinline__ int64_t last(int j) const {
     return j + 1 < njobs ? jobs[j + 1].block_start : nbands;
   }
-  __device__ __forceinline__ void range(int c, int, int64_t &b0, int64_t &b1) const {
-    b0 = band_start[c];
-    b1 = band_start[c + 1];
-  }
 };
 
 template <int KIND>
 __global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
-    oz_pack_fused_grouped(const PackJob *jobs, const int *band_start, int njobs, int nbands) {
+    oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
   extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk<KIND>(GroupBands{jobs, band_start, njobs, nbands}, pack_ring,
+  oz_pack_walk<KIND>(GroupBands{jobs, njobs, nbands}, pack_ring,
                      reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(pack_ring) + kPackRingBytes));
 }
 
@@ -2233,21 +2227,7 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
       if (pack_kind_of(j.pa) != g.pack_kind) g.pack_kind = kPackAny;
   }
   g.tiles = tiles.back();
-  // Fused pack: each CTA's contiguous band range, balanced by tile steps.
-  std::vector<int> bstart;
-  if (oz && blocks > 0) {
-    g.pack_grid = (int)std::min<int64_t>(blocks, (int64_t)kPackCtasPerSm * num_sms());
-    std::vector<int64_t> nb(jobs.size()), st(jobs.size());
-    int64_t T = 0;
-    for (size_t j = 0; j < jobs.size(); ++j) {
-      nb[j] = jobs[j].gx;
-      st[j] = band_nk1(jobs[j].pa.K) + band_nk2(jobs[j].pa.kblocks);
-      T += nb[j] * st[j];
-    }
-    bstart.resize((size_t)g.pack_grid + 1);
-    for (int c = 0; c <= g.pack_grid; ++c)
-      bstart[(size_t)c] = (int)band_at_step(T * c / g.pack_grid, (int)jobs.size(), nb.data(), st.data());
-  }
+  if (oz && blocks > 0) g.pack_grid = (int)std::min<int64_t>(blocks, (int64_t)kPackCtasPerSm * num_sms());
   size_t off = 0;
   g.off_pack = off;
   off = align_up(off + jobs.size() * sizeof(PackJob), 64);
@@ -2259,8 +2239,6 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   off = align_up(off + zero.size() * sizeof(ZeroJob), 64);
   g.off_fix = off;
   off = align_up(off + fix.size() * sizeof(FixupJob), 64);
-  g.off_bstart = off;
-  off = align_up(off + bstart.size() * sizeof(int), 64);
   g.image.assign(off, 0);
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes) std::memcpy(g.image.data() + at, src, bytes);
@@ -2270,7 +2248,6 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   put(g.off_tiles, tiles.data(), tiles.size() * sizeof(int));
   put(g.off_zero, zero.data(), zero.size() * sizeof(ZeroJob));
   put(g.off_fix, fix.data(), fix.size() * sizeof(FixupJob));
-  put(g.off_bstart, bstart.data(), bstart.size() * sizeof(int));
   return QS_OK;
 }
 
@@ -2316,21 +2293,20 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
     static std::atomic<int> done[3];
     const int pgrid2 = g.pack_grid;
-    const int *bstart = (const int *)(d + g.off_bstart);
     switch (pgrid2 > 0 ? g.pack_kind : -1) {
       case -1:
         break;
       case kPackF64:
         pack_smem_attr(oz_pack_fused_grouped<kPackF64>, done[0]);
-        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
       case kPackF32:
         pack_smem_attr(oz_pack_fused_grouped<kPackF32>, done[1]);
-        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
       default:
         pack_smem_attr(oz_pack_fused_grouped<kPackAny>, done[2]);
-        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, bstart, g.njobs, g.pack_blocks);
+        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
         break;
     }
     if (g.cls == TC_CLASS_OZ4)
