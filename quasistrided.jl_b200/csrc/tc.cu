@@ -442,11 +442,24 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   const int s = a.nslices;
   if (t < nk1) {
     if (t == 0) bs.mb = 0;
+    if constexpr (KIND == kPackF32) {
+      // |x| orders as its Float32 bit pattern: one conversion per lane and tile
+      uint32_t m32 = 0;
 #pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
-      const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
+      for (int kk = 0; kk < 16; ++kk) {
+        const int k = lane * 16 + kk;
+        const uint32_t b = *reinterpret_cast<const uint32_t *>(tile + w * kBandStride + band_col(k)) & 0x7FFFFFFFu;
+        m32 = b > m32 ? b : m32;
+      }
+      const unsigned long long b = (unsigned long long)__double_as_longlong((double)__uint_as_float(m32));
       bs.mb = b > bs.mb ? b : bs.mb;
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk) {
+        const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
+        bs.mb = b > bs.mb ? b : bs.mb;
+      }
     }
     if (t == nk1 - 1) {
 #pragma unroll
@@ -487,16 +500,30 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   // value scaled by f and rounded once to an integer, |q| <= 127 * 2^(8s-8);
   // the bytes of q + 0x80..80 (s bytes) are the digits + 128, low digit
   // first.
+  // For s <= 6, |q| < 2^47: one FMA with 1.5 * 2^52 rounds the exact v * f
+  // to the integer q (ties to even) and leaves 2^51 + q in the low 52 bits of
+  // its bit pattern, so the low 8s bits of those bits + (bias - 2^51) are
+  // q + bias (one FP64 operation and one 64-bit add; a float-to-integer
+  // conversion runs on the quarter-rate conversion pipe).  s = 7 needs 56
+  // bits and converts.
   const unsigned long long bias = 0x8080808080808080ull >> (64 - 8 * s);
+  constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+  const unsigned long long mbias = bias - (1ull << 51);
+  const bool magic = s <= 6;
   uint32_t lo[16], hi[16];
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) {
-    double y = 0.0;
+    unsigned long long u = bias;  // digits of 0
     if (!zero) {
       const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
-      y = bs.wide ? scale2(v, -bs.E) * bs.f : v * bs.f;
+      if (magic) {
+        const double tt = bs.wide ? __dadd_rn(__dmul_rn(scale2(v, -bs.E), bs.f), kMagic) : __fma_rn(v, bs.f, kMagic);
+        u = (unsigned long long)__double_as_longlong(tt) + mbias;
+      } else {
+        const double y = bs.wide ? scale2(v, -bs.E) * bs.f : v * bs.f;
+        u = (unsigned long long)__double2ll_rn(y) + bias;
+      }
     }
-    const unsigned long long u = (unsigned long long)__double2ll_rn(y) + bias;
     lo[kk] = (uint32_t)u;
     hi[kk] = (uint32_t)(u >> 32);
   }
