@@ -172,7 +172,7 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-STAGE_NAMES = {"ozaki": ["pack", "pack_none", "gemm_i8", "fixup"],
+STAGE_NAMES = {"ozaki": ["pack_a", "pack_b", "gemm_i8", "fixup"],
                "bf16x3": ["pack", "pack_none", "gemm_bf16"],
                "native": ["gemm_native"]}
 

@@ -76,8 +76,6 @@ struct Workspace {
   int64_t *offM[2] = {nullptr, nullptr};
   int64_t *offN[2] = {nullptr, nullptr};
   int64_t *offK[2] = {nullptr, nullptr};
-  // Ozaki pack: the K maps as int32 (staged in shared memory), or nullptr
-  int32_t *offK32[2] = {nullptr, nullptr};
   // batch labels: [A offsets | B offsets | C offsets], P each, or nullptr
   int64_t *offBatch = nullptr;
   // tensor-core paths: packed operand panels and per-row/col exponents
@@ -85,6 +83,7 @@ struct Workspace {
   void *panelB = nullptr;
   int32_t *expA = nullptr;  // per packed row of A (Ozaki), or nullptr
   int32_t *expB = nullptr;
+  unsigned long long *rowmax = nullptr;  // Ozaki: row maxima of A (Mp) then B (Np)
   int32_t *status = nullptr;  // device status word (bounded waits)
   size_t bytes = 0;
   std::vector<void *> owned;         // every allocated block, for freeing

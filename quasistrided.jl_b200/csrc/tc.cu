@@ -74,9 +74,9 @@ struct PackArgs {
   // `rows`/`K` above are the real (virtual) extents; offR/offK index the
   // complex elements.
   int cmode;
-  // Real operands (cmode 0): the K offsets as int32 (K entries, padded to a
-  // multiple of 4) when K <= kStageK and every offset fits, else nullptr.
-  const int32_t *offK32;
+  // Ozaki pass 1 -> pass 2: each padded row's max |x| bit pattern (zeroed
+  // before every pack), or nullptr.
+  unsigned long long *rowmax;
 };
 
 // Element (r, k) of the real (virtual) matrix the panels hold.
@@ -225,46 +225,20 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
   }
 }
 
-// Fused Ozaki pack: both passes in one launch, each operand read once from
-// HBM.  A CTA walks a contiguous range of bands of kBandRows (virtual) rows;
-// the ranges are balanced by tile steps.  Phase 1 streams a band's K tiles
-// and reduces every row's max |x| bit pattern in registers (no atomics,
-// nothing to clear per execute); phase 2 streams the band again and emits
-// the digit planes.  Three CTAs per SM keep the bands in flight
-// (kBandRows * K * 8 bytes each) small enough to stay in L2 between the two
-// phases, so phase 2 reads them from there.
-//
-// The tiles move by cp.async into a kPackBufs-deep ring, kPackBufs - 1
-// tiles ahead of the one being processed and across band boundaries, so
-// every CTA keeps a tile of loads in flight (a pack with synchronous loads
-// left HBM at 8 % of its bandwidth).  The copies are raw element bytes: a
-// tile slot holds one real value or one complex component (Float32 in its
-// low four bytes), and the virtual matrix (type conversion, conj, the 1e /
-// 1r complex layouts) is formed when a slot is read.  A real operand's K
-// offsets sit in shared memory as int32 (staged once per operand when
-// K <= kStageK and they fit), so forming a copy's address reads no global
-// memory.
-constexpr int kBandRows = 4, kBandK = 512, kPackBufs = 3;
-constexpr int kPackThreads = 32 * kBandRows;  // a warp per row
-constexpr int kPackCtasPerSm = 3;
-constexpr int kBandStride = kBandK + kBandK / 16 + 4;  // +1 slot per 16, +4 per row: conflict-free
-constexpr int kStageK = 4608;                          // K offsets staged in shared memory
-constexpr size_t kPackRingBytes = (size_t)kPackBufs * kBandRows * kBandStride * 8;
-constexpr size_t kPackSmem = kPackRingBytes + (size_t)kStageK * sizeof(int32_t);
+// Ozaki pack in two streaming passes per operand.  Pass 1 (oz_rowmax_block)
+// reduces every row's max |x| bit pattern into a zeroed workspace (one
+// atomicMax per row and block); pass 2 (oz_digit_block) derives the row's
+// exponent from it and writes the digit planes.  Blocks are 32 rows x 128 K
+// values: a thread's 16 loads are independent and in flight together, and
+// six (pass 1) or four (pass 2, which holds 32 words of digit bytes per
+// thread) blocks per SM keep 130-200 KB of loads outstanding.  The plan runs the
+// passes operand by operand, so the second pass re-reads an operand that
+// the first has just brought into L2.
+constexpr int kPackRows = 32, kPackK = 128;
 
-__device__ __forceinline__ int band_col(int k) { return k + (k >> 4); }
-
-// No "memory" clobber (as cp_async8): loop-invariant loads stay in registers.
-__device__ __forceinline__ void cp_async_4_8(uint32_t saddr, const void *g, int size, bool ok) {
-  if (size == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 8 : 0));
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(g), "r"(ok ? 4 : 0));
-}
-
-// Element kinds of a pack walk, fixed per launch: real Float64 or real
-// Float32 operands take straight-line copies with their row offsets hoisted
-// per band; anything else (complex layouts, mixed types) the general path.
+// Element kinds, fixed per launch: real Float64 or real Float32 operands
+// take the straight-line loads of load_tile_real; anything else (complex
+// layouts, mixed types) the general loader.
 enum { kPackF64 = 0, kPackF32 = 1, kPackAny = 2 };
 
 __host__ __device__ inline int pack_kind_of(const PackArgs &a) {
@@ -273,260 +247,107 @@ __host__ __device__ inline int pack_kind_of(const PackArgs &a) {
   return kPackAny;
 }
 
-// The issue cursor's row offsets (element index of column 0 of each row the
-// thread copies; INT64_MIN outside the operand): rfast threads use ro[0]
-// (their one row), K-fast threads all kBandRows rows.
-struct IssueRows {
-  int64_t ro[kBandRows];
-};
-
 template <int KIND>
-__device__ __forceinline__ void band_seat_rows(const PackArgs &a, int64_t r0, IssueRows &ir) {
-  if constexpr (KIND != kPackAny) {
-    if (a.rfast) {
-      const int64_t r = r0 + threadIdx.x % kBandRows;
-      ir.ro[0] = r < a.rows ? a.Xbase + __ldg(a.offR + r) : INT64_MIN;
-    } else {
-#pragma unroll
-      for (int rr = 0; rr < kBandRows; ++rr) {
-        const int64_t r = r0 + rr;
-        ir.ro[rr] = r < a.rows ? a.Xbase + __ldg(a.offR + r) : INT64_MIN;
-      }
-    }
-  }
+__device__ __forceinline__ void pack_load(const PackArgs &a, int64_t r0, int64_t k0,
+                                          double (*tile)[kPackK + 1]) {
+  if constexpr (KIND == kPackF64) load_tile_real<double, double, kPackK>(a, r0, k0, tile);
+  else if constexpr (KIND == kPackF32) load_tile_real<double, float, kPackK>(a, r0, k0, tile);
+  else load_tile<double, kPackK>(a, r0, k0, tile);
 }
 
-// K offset of index k: from the staged shared-memory table, or from global
-// memory.
-struct SmemKoff {
-  const int32_t *t;
-  __device__ __forceinline__ int64_t operator()(int64_t k) const { return t[k]; }
-};
-struct GlobalKoff {
-  const int64_t *__restrict__ t;
-  __device__ __forceinline__ int64_t operator()(int64_t k) const { return __ldg(t + k); }
-};
-
-// The copies of a real operand's K tile [k0, k0 + kBandK) (element size ESZ).
-template <int ESZ, class Koff>
-__device__ __forceinline__ void band_issue_real(const PackArgs &a, int64_t k0, uint32_t tile, const IssueRows &ir,
-                                                Koff koff) {
-  const int tid = threadIdx.x;
-  const char *X = static_cast<const char *>(a.X);
-  const int64_t K = a.K;
-  if (a.rfast) {
-    const int rr = tid % kBandRows, kb = tid / kBandRows;
-    const int64_t ro = ir.ro[0];
-#pragma unroll
-    for (int i = 0; i < kBandK / (kPackThreads / kBandRows); ++i) {
-      const int kk = kb + (kPackThreads / kBandRows) * i;
-      const int64_t k = k0 + kk;
-      const bool ok = ro != INT64_MIN && k < K;
-      const char *src = ok ? X + (ro + koff(k)) * ESZ : X;
-      cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
-    }
-  } else {
-#pragma unroll
-    for (int h = 0; h < kBandK / kPackThreads; ++h) {
-      const int kk = tid + kPackThreads * h;
-      const int64_t k = k0 + kk;
-      const bool kok = k < K;
-      const int64_t ko = kok ? koff(k) : 0;
-#pragma unroll
-      for (int rr = 0; rr < kBandRows; ++rr) {
-        const bool ok = kok && ir.ro[rr] != INT64_MIN;
-        const char *src = ok ? X + (ir.ro[rr] + ko) * ESZ : X;
-        cp_async_4_8(tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk)), src, ESZ, ok);
-      }
-    }
-  }
-}
-
-// Issue the copies of K tile [k0, k0 + kBandK) of virtual rows
-// [r0, r0 + kBandRows) into `tile` (slot (row, k) at row * kBandStride +
-// band_col(k)), zero-filled outside the operand, coalesced along X's
-// unit-stride axis.  Real operands: slot = element, K offsets from `skoff`
-// (the staged table) when it is not null.  General path: 1r (cmode 2, K
-// doubled): slots 2j, 2j+1 = re, im of complex K index j; 1e (cmode 1, rows
-// and K doubled): complex row i goes to even row 2i as in 1r and odd rows are
-// formed from it on read; a real operand in a complex layout gets zero
-// imaginary slots.
+// Pass 1: each row's max magnitude as the bit pattern of |x| (for
+// non-negative doubles the integer order is the value order, and a NaN or
+// Inf sorts above every finite value).  8 threads per row.
 template <int KIND>
-__device__ __forceinline__ void band_issue(const PackArgs &a, int64_t r0, int64_t k0, uint32_t tile,
-                                           const IssueRows &ir, const int32_t *skoff) {
-  if constexpr (KIND != kPackAny) {
-    constexpr int ESZ = KIND == kPackF64 ? 8 : 4;
-    if (skoff) band_issue_real<ESZ>(a, k0, tile, ir, SmemKoff{skoff});
-    else band_issue_real<ESZ>(a, k0, tile, ir, GlobalKoff{a.offK});
-    return;
+__device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, int64_t r0, int64_t k0) {
+  __shared__ double tile[kPackRows][kPackK + 1];
+  pack_load<KIND>(a, r0, k0, tile);
+  __syncthreads();
+  const int row = threadIdx.x >> 3, part = threadIdx.x & 7;
+  unsigned long long m = 0;
+#pragma unroll
+  for (int kk = 0; kk < 16; ++kk) {
+    const unsigned long long b =
+        (unsigned long long)__double_as_longlong(fabs(tile[row][tcol<kPackK>(part * 16 + kk)]));
+    m = b > m ? b : m;
   }
-  const int tid = threadIdx.x;
-  const char *X = static_cast<const char *>(a.X);
-  const int64_t K = a.K;
-  const int64_t *__restrict__ offK = a.offK;
-  const bool cx = a.TX == QS_C32 || a.TX == QS_C64;
-  const int esz = (a.TX == QS_F64 || a.TX == QS_C64) ? 8 : 4;
-  const int cmode = a.cmode;
-  const int64_t rows = a.rows, Xbase = a.Xbase;
-  const int64_t *__restrict__ offR = a.offR;
-  auto slot = [&](int rr, int kk) {
-    const int64_t r = r0 + rr, k = k0 + kk;
-    const uint32_t dst = tile + 8u * (uint32_t)(rr * kBandStride + band_col(kk));
-    if (cmode == 1 && (rr & 1)) return;  // derived from the even row
-    bool ok = r < rows && k < K;
-    const int64_t rix = cmode == 1 ? (r >> 1) : r, kix = cmode ? (k >> 1) : k;
-    const int part = cmode ? (int)(k & 1) : 0;
-    if (part && !cx) ok = false;  // imaginary part of a real operand
-    const char *src = X;
-    if (ok) {
-      const int64_t e = Xbase + __ldg(offR + rix) + __ldg(offK + kix);
-      src = X + (cx ? (2 * e + part) : e) * esz;
-    }
-    cp_async_4_8(dst, src, esz, ok);
-  };
-  constexpr int PER = kBandRows * kBandK / kPackThreads;
-  if (a.rfast) {
-#pragma unroll 4
-    for (int i = 0; i < PER; ++i) slot(tid % kBandRows, tid / kBandRows + (kPackThreads / kBandRows) * i);
-  } else {
-#pragma unroll 4
-    for (int i = 0; i < PER; ++i) slot(i % kBandRows, tid + kPackThreads * (i / kBandRows));
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
   }
+  if (part == 0 && r0 + row < a.rows && m) atomicMax(a.rowmax + r0 + row, m);
 }
 
-// Virtual value (row w, K index kk) of a staged tile.
-template <int KIND>
-__device__ __forceinline__ double band_value(const PackArgs &a, const double *tile, int w, int kk) {
-  auto raw = [&](int row, int k) -> double {
-    const double *p = tile + row * kBandStride + band_col(k);
-    if constexpr (KIND == kPackF64) return *p;
-    if constexpr (KIND == kPackF32) return (double)*reinterpret_cast<const float *>(p);
-    if (a.TX == QS_F64 || a.TX == QS_C64) return *p;
-    return (double)*reinterpret_cast<const float *>(p);
-  };
-  if constexpr (KIND != kPackAny) {
-    return raw(w, kk);
-  } else {
-    if (a.cmode == 0) return raw(w, kk);
-    if (a.cmode == 2) {
-      const double v = raw(w, kk);
-      return ((kk & 1) && a.conj) ? -v : v;
-    }
-    const int base = w & ~1;
-    const double re = raw(base, kk & ~1);
-    double im = raw(base, kk | 1);
-    if (a.conj) im = -im;
-    const int rp = w & 1, kp = kk & 1;
-    return rp == kp ? re : (rp ? im : -im);
-  }
-}
-
-// One row band's state for the processing side.
-struct BandState {
-  unsigned long long mb;  // running max |x| bit pattern of this warp's row
+// The row's exponent E (frexp exponent of the max + 1; kNonFinite for a row
+// holding a NaN or Inf, 0 for a zero row) and digit scale
+// f = 127/128 * 2^(8s - E) (wide: 127/128 * 2^(8s), after an exact scale by
+// 2^-E).
+struct RowScale {
   int E;
-  bool bad;
-  bool wide;  // 2^(8s - E) is outside the normal range: scale in two steps
-  double f;   // the digit scale 127/128 * 2^(8s - E) (wide: 127/128 * 2^(8s))
+  bool bad, zero, wide;
+  double f;
 };
-
-// Process tile `t` (phase 1: t < nk1; phase 2 otherwise) of the band at
-// r0: warp w owns virtual row r0 + w, lane l its K values 16 l .. 16 l + 15.
-// Loaded tiles are zero-filled past K; phase-2 tiles past K are not loaded
-// and read as zeros.
-template <int KIND>
-__device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int t, int nk1, const double *tile,
-                                             BandState &bs) {
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t grow = r0 + w;
-  const int s = a.nslices;
-  if (t < nk1) {
-    if (t == 0) bs.mb = 0;
-    if constexpr (KIND == kPackF32) {
-      // |x| orders as its Float32 bit pattern: one conversion per lane and tile
-      uint32_t m32 = 0;
-#pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        const int k = lane * 16 + kk;
-        const uint32_t b = *reinterpret_cast<const uint32_t *>(tile + w * kBandStride + band_col(k)) & 0x7FFFFFFFu;
-        m32 = b > m32 ? b : m32;
-      }
-      const unsigned long long b = (unsigned long long)__double_as_longlong((double)__uint_as_float(m32));
-      bs.mb = b > bs.mb ? b : bs.mb;
-    } else {
-#pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
-        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v));
-        bs.mb = b > bs.mb ? b : bs.mb;
-      }
-    }
-    if (t == nk1 - 1) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long x = __shfl_xor_sync(0xffffffffu, bs.mb, o);
-        bs.mb = x > bs.mb ? x : bs.mb;
-      }
-      // E: the row max's frexp exponent + 1; non-finite rows get kNonFinite,
-      // zero digits and a place on the fixup list.
-      bs.E = 0;
-      bs.bad = bs.mb >= 0x7FF0000000000000ull;
-      bs.wide = false;
-      bs.f = 0.0;
-      if (bs.bad) {
-        bs.E = kNonFinite;
-      } else if (bs.mb) {
-        frexp(__longlong_as_double((long long)bs.mb), &bs.E);
-        bs.E += 1;
-        const int sh = 8 * s - bs.E;
-        bs.wide = sh < -1000 || sh > 1000;
-        bs.f = kDigitScale * __longlong_as_double((long long)((bs.wide ? 8 * s : sh) + 1023) << 52);
-      }
-      if (grow < a.rows_pad && lane == 0) {
-        a.exp_out[grow] = bs.E;
-        if (bs.bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
-      }
-    }
-    return;
+__device__ __forceinline__ RowScale row_scale(unsigned long long mb, int s) {
+  RowScale r{0, mb >= 0x7FF0000000000000ull, mb == 0, false, 0.0};
+  if (r.bad) {
+    r.E = kNonFinite;
+  } else if (!r.zero) {
+    frexp(__longlong_as_double((long long)mb), &r.E);
+    r.E += 1;
+    const int sh = 8 * s - r.E;
+    r.wide = sh < -1000 || sh > 1000;
+    r.f = kDigitScale * __longlong_as_double((long long)((r.wide ? 8 * s : sh) + 1023) << 52);
   }
-  const int64_t k0 = (int64_t)(t - nk1) * kBandK;
-  const int64_t kpad = (int64_t)a.kblocks * kKBytes;  // digits per row (bytes = K values)
-  const int64_t kc = k0 + lane * 16;
-  if (grow >= a.rows_pad || kc >= kpad) return;
-  const bool zero = bs.bad || !bs.mb || k0 >= a.K;
-  const int64_t plane = a.plane;
-  uint8_t *dst = a.panel + panel_tile_base(a, grow, kc);
-  // Digits (the balanced base-256 expansion described above): q = the row's
-  // value scaled by f and rounded once to an integer, |q| <= 127 * 2^(8s-8);
+  return r;
+}
+
+// Pass 2: the digit planes of one 32-row x 128-K block (the balanced
+// base-256 digits described above).  Thread (row, c) writes the 16 digits
+// of K values c*16 .. c*16 + 15 of its row into each plane.
+template <int KIND>
+__device__ __forceinline__ void oz_digit_block(const PackArgs &a, int64_t r0, int64_t k0) {
+  __shared__ double tile[kPackRows][kPackK + 1];
+  pack_load<KIND>(a, r0, k0, tile);
+  __syncthreads();
+  const int row = threadIdx.x >> 3, c = threadIdx.x & 7;
+  const int64_t grow = r0 + row;
+  if (grow >= a.rows_pad) return;
+  const int s = a.nslices;
+  const RowScale rs = row_scale(grow < a.rows ? __ldg(a.rowmax + grow) : 0ull, s);
+  if (k0 == 0 && c == 0) {
+    a.exp_out[grow] = rs.E;
+    if (rs.bad) a.flag_list[atomicAdd(a.flag_count, 1)] = (int32_t)grow;
+  }
+  // q = the value times f rounded once to an integer, |q| <= 127 * 2^(8s-8);
   // the bytes of q + 0x80..80 (s bytes) are the digits + 128, low digit
-  // first.
-  // For s <= 6, |q| < 2^47: one FMA with 1.5 * 2^52 rounds the exact v * f
-  // to the integer q (ties to even) and leaves 2^51 + q in the low 52 bits of
-  // its bit pattern, so the low 8s bits of those bits + (bias - 2^51) are
-  // q + bias (one FP64 operation and one 64-bit add; a float-to-integer
-  // conversion runs on the quarter-rate conversion pipe).  s = 7 needs 56
-  // bits and converts.
+  // first.  For s <= 6, |q| < 2^47: one FMA with 1.5 * 2^52 rounds the exact
+  // v * f to q (ties to even) and leaves 2^51 + q in the low 52 bits of its
+  // bit pattern, so the low 8s bits of those bits + (bias - 2^51) are
+  // q + bias.  s = 7 needs 56 bits and converts.
   const unsigned long long bias = 0x8080808080808080ull >> (64 - 8 * s);
   constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
   const unsigned long long mbias = bias - (1ull << 51);
-  const bool magic = s <= 6;
+  const bool live = !rs.bad && !rs.zero;
   uint32_t lo[16], hi[16];
 #pragma unroll
   for (int kk = 0; kk < 16; ++kk) {
-    unsigned long long u = bias;  // digits of 0
-    if (!zero) {
-      const double v = band_value<KIND>(a, tile, w, lane * 16 + kk);
-      if (magic) {
-        const double tt = bs.wide ? __dadd_rn(__dmul_rn(scale2(v, -bs.E), bs.f), kMagic) : __fma_rn(v, bs.f, kMagic);
-        u = (unsigned long long)__double_as_longlong(tt) + mbias;
+    unsigned long long u = bias;  // the digits of 0
+    if (live) {
+      const double v = tile[row][tcol<kPackK>(c * 16 + kk)];
+      if (s <= 6) {
+        const double t = rs.wide ? __dadd_rn(__dmul_rn(scale2(v, -rs.E), rs.f), kMagic) : __fma_rn(v, rs.f, kMagic);
+        u = (unsigned long long)__double_as_longlong(t) + mbias;
       } else {
-        const double y = bs.wide ? scale2(v, -bs.E) * bs.f : v * bs.f;
+        const double y = rs.wide ? scale2(v, -rs.E) * rs.f : v * rs.f;
         u = (unsigned long long)__double2ll_rn(y) + bias;
       }
     }
     lo[kk] = (uint32_t)u;
     hi[kk] = (uint32_t)(u >> 32);
   }
+  uint8_t *dst = a.panel + panel_tile_base(a, grow, k0 + c * 16);
+  const int64_t plane = a.plane;
   for (int p = 0; p < s; ++p) {
     // plane p holds digit p + 1 (weight 256^-(p+1)): byte s - 1 - p of q + bias
     const int bi = s - 1 - p;
@@ -547,178 +368,44 @@ __device__ __forceinline__ void band_process(const PackArgs &a, int64_t r0, int 
   }
 }
 
-// Steps of one band: nk1 tiles of phase 1, nk2 of phase 2.
-__host__ __device__ inline int band_nk1(int64_t K) { return (int)((K + kBandK - 1) / kBandK); }
-__host__ __device__ inline int band_nk2(int kblocks) { return (int)(((int64_t)kblocks * kKBytes + kBandK - 1) / kBandK); }
-
-// A walk over this CTA's bands b = blockIdx.x + n * gridDim.x (neighbouring
-// bands in neighbouring CTAs, so the rows of an M-fast operand that share a
-// DRAM burst are read at about the same time), one tile step at a time:
-// steps 0 .. nk1 + nk2 - 1 per band (phase-2 tiles past K load nothing).
-// `Bands` maps band indices to jobs (one operand of one problem: its
-// PackArgs and first band); the cursor follows the job index forward.  Each
-// band's PackArgs is copied into one of the cursor's two shared-memory
-// slots, so the loops read shared memory rather than the parameter or job
-// table through a runtime-selected pointer.
-template <class Bands>
-struct BandCursor {
-  int64_t b;
-  int t;
-  int job;
-  int64_t jfirst, jend;
-  PackArgs *slots;  // two shared-memory slots, alternating per band
-  int par;
-  const PackArgs *a;
-  int64_t r0;
-  int nk1, nk2;
-  __device__ __forceinline__ void start(const Bands &bands, PackArgs *s2) {
-    b = blockIdx.x;
-    t = 0;
-    slots = s2;
-    par = 0;
-    if (b < bands.count()) {
-      job = bands.find(b);
-      enter(bands);
-    }
-  }
-  // Copies the job's PackArgs (every thread of the CTA calls it; the copy is
-  // read after the next __syncthreads).
-  __device__ __forceinline__ void enter(const Bands &bands) {
-    const PackArgs *src = bands.args(job);
-    par ^= 1;
-    uint64_t *d = reinterpret_cast<uint64_t *>(&slots[par]);
-    const uint64_t *s = reinterpret_cast<const uint64_t *>(src);
-    for (int i = threadIdx.x; i < (int)(sizeof(PackArgs) / 8); i += kPackThreads) d[i] = s[i];
-    a = &slots[par];
-    jfirst = bands.first(job);
-    jend = bands.last(job);
-    nk1 = band_nk1(src->K);
-    nk2 = band_nk2(src->kblocks);
-    r0 = (b - jfirst) * kBandRows;
-  }
-  __device__ __forceinline__ const PackArgs *source(const Bands &bands) const { return bands.args(job); }
-  __device__ __forceinline__ bool valid(const Bands &bands) const { return b < bands.count(); }
-  // Advances one step; true when it moved to a new band.
-  __device__ __forceinline__ bool next(const Bands &bands) {
-    if (++t < nk1 + nk2) return false;
-    t = 0;
-    b += gridDim.x;
-    if (b < bands.count()) {
-      if (b >= jend) {
-        do ++job;
-        while (bands.last(job) <= b);
-      }
-      enter(bands);
-    }
-    return true;
-  }
-};
-static_assert(sizeof(PackArgs) % 8 == 0, "PackArgs copies as 8-byte words");
-
-template <int KIND, class Bands>
-__device__ __forceinline__ void oz_pack_walk(const Bands &bands, double *ring, int32_t *skoff) {
-  __shared__ PackArgs s_args[4];  // [issue cursor: 2][process cursor: 2]
-  const uint32_t ring_u32 = smem_u32(ring);
-  constexpr uint32_t kTileBytes = kBandRows * kBandStride * 8;
-  BandCursor<Bands> in, out;
-  in.start(bands, s_args);
-  out.start(bands, s_args + 2);
-  IssueRows ir;
-  if (in.valid(bands)) band_seat_rows<KIND>(*in.source(bands), in.r0, ir);
-  __syncthreads();  // the first slots are filled
-  int staged = -1;  // the job whose K offsets are in skoff
-  uint32_t issued = 0, done = 0;
-  auto issue = [&]() {
-    if (in.valid(bands)) {
-      const int32_t *ko = nullptr;
-      if constexpr (KIND != kPackAny) {
-        if (in.a->offK32) {
-          if (in.job != staged) {
-            // Uniform over the CTA (one cursor): no thread reads the old
-            // table past the first barrier.
-            __syncthreads();
-            const int n4 = (int)((in.a->K + 3) >> 2);
-            const int4 *src = reinterpret_cast<const int4 *>(in.a->offK32);
-            for (int i = threadIdx.x; i < n4; i += kPackThreads) reinterpret_cast<int4 *>(skoff)[i] = __ldg(src + i);
-            __syncthreads();
-            staged = in.job;
-          }
-          ko = skoff;
-        }
-      }
-      const int64_t k0 = (int64_t)(in.t < in.nk1 ? in.t : in.t - in.nk1) * kBandK;
-      if (k0 < in.a->K) band_issue<KIND>(*in.a, in.r0, k0, ring_u32 + (issued % kPackBufs) * kTileBytes, ir, ko);
-      if (in.next(bands) && in.valid(bands)) band_seat_rows<KIND>(*in.source(bands), in.r0, ir);
-    }
-    cp_async_commit();
-    ++issued;
-  };
-  for (int q = 0; q < kPackBufs - 1; ++q) {
-    issue();
-    __syncthreads();  // a slot the issue filled is read by the next one
-  }
-  BandState bs{0, 0, false, false, 0.0};
-  while (out.valid(bands)) {
-    cp_async_wait<kPackBufs - 2>();  // this step's tile has landed (for this thread)
-    __syncthreads();                 // ... for every thread; the oldest buffer is free again
-    issue();
-    band_process<KIND>(*out.a, out.r0, out.t, out.nk1,
-                       ring + (size_t)(done % kPackBufs) * kBandRows * kBandStride, bs);
-    ++done;
-    out.next(bands);
-  }
-  cp_async_wait<0>();
+// One operand of one plan: blocks (row block fastest, then K block).
+__device__ __forceinline__ void pack_block_coords(int64_t b, int nrb, int64_t &r0, int64_t &k0) {
+  r0 = (b % nrb) * kPackRows;
+  k0 = (b / nrb) * kPackK;
 }
-
-// Both operands of one plan: bands [0, nbA) of A, then [0, nbB) of B.
-struct PairBands {
-  const PackArgs *pa, *pb;
-  int64_t nbA, nbB;
-  __device__ __forceinline__ int64_t count() const { return nbA + nbB; }
-  __device__ __forceinline__ int find(int64_t b) const { return b < nbA ? 0 : 1; }
-  __device__ __forceinline__ const PackArgs *args(int j) const { return j == 0 ? pa : pb; }
-  __device__ __forceinline__ int64_t first(int j) const { return j == 0 ? 0 : nbA; }
-  __device__ __forceinline__ int64_t last(int j) const { return j == 0 ? nbA : nbA + nbB; }
-};
 
 template <int KIND>
-__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
-    oz_pack_fused_kernel(const __grid_constant__ PackArgs pa, const __grid_constant__ PackArgs pb, int64_t nbA,
-                         int64_t nbB) {
-  extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk<KIND>(PairBands{&pa, &pb, nbA, nbB}, pack_ring,
-                     reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(pack_ring) + kPackRingBytes));
+__global__ void __launch_bounds__(256, 6) oz_rowmax_kernel(const __grid_constant__ PackArgs a, int nrb) {
+  int64_t r0, k0;
+  pack_block_coords(blockIdx.x, nrb, r0, k0);
+  oz_rowmax_block<KIND>(a, r0, k0);
 }
 
-// The kind both operands share, else the general path.
-static int pack_kind(const PackArgs &pa, const PackArgs &pb) {
-  const int ka = pack_kind_of(pa), kb = pack_kind_of(pb);
-  return ka == kb ? ka : kPackAny;
+template <int KIND>
+__global__ void __launch_bounds__(256, 4) oz_digit_kernel(const __grid_constant__ PackArgs a, int nrb) {
+  int64_t r0, k0;
+  pack_block_coords(blockIdx.x, nrb, r0, k0);
+  oz_digit_block<KIND>(a, r0, k0);
 }
 
-template <class K>
-static void pack_smem_attr(K kernel, std::atomic<int> &done) {
-  if (!done.load()) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPackSmem);
-    done.store(1);
-  }
-}
-
-static cudaError_t launch_pack_fused(const PackArgs &pa, const PackArgs &pb, int64_t nbA, int64_t nbB, int grid,
-                                     cudaStream_t st) {
-  static std::atomic<int> done[3];
-  switch (pack_kind(pa, pb)) {
+// Pass 1 and pass 2 of one operand: blocks cover rows_pad x kblocks * 128
+// (pass 1 only needs K, pass 2 writes the zero padding of K too).
+static cudaError_t launch_pack_operand(const PackArgs &a, cudaStream_t st) {
+  const int nrb = (int)((a.rows_pad + kPackRows - 1) / kPackRows);
+  const unsigned n1 = (unsigned)((int64_t)nrb * ((a.K + kPackK - 1) / kPackK));
+  const unsigned n2 = (unsigned)((int64_t)nrb * a.kblocks);
+  switch (pack_kind_of(a)) {
     case kPackF64:
-      pack_smem_attr(oz_pack_fused_kernel<kPackF64>, done[0]);
-      oz_pack_fused_kernel<kPackF64><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_rowmax_kernel<kPackF64><<<n1, 256, 0, st>>>(a, nrb);
+      oz_digit_kernel<kPackF64><<<n2, 256, 0, st>>>(a, nrb);
       break;
     case kPackF32:
-      pack_smem_attr(oz_pack_fused_kernel<kPackF32>, done[1]);
-      oz_pack_fused_kernel<kPackF32><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_rowmax_kernel<kPackF32><<<n1, 256, 0, st>>>(a, nrb);
+      oz_digit_kernel<kPackF32><<<n2, 256, 0, st>>>(a, nrb);
       break;
     default:
-      pack_smem_attr(oz_pack_fused_kernel<kPackAny>, done[2]);
-      oz_pack_fused_kernel<kPackAny><<<grid, kPackThreads, kPackSmem, st>>>(pa, pb, nbA, nbB);
+      oz_rowmax_kernel<kPackAny><<<n1, 256, 0, st>>>(a, nrb);
+      oz_digit_kernel<kPackAny><<<n2, 256, 0, st>>>(a, nrb);
       break;
   }
   return cudaGetLastError();
@@ -1804,30 +1491,6 @@ static bool make_pair_maps(qs_plan *p) {
   return true;
 }
 
-// The int32 copy of a real operand's K map for the fused pack's staged
-// table: only when the operand is real (no complex layout), K <= kStageK and
-// every offset fits in int32; else the pack reads the int64 map.
-static int upload_koff32(qs_plan *p, int side) {
-  const TensorCoreGeom &g = p->tc;
-  const int T = side == 0 ? p->TA : p->TB;
-  if (g.cplx_layout != 0 || is_complex(T) || p->K <= 0 || p->K > kStageK) return QS_OK;
-  int64_t lo, hi;
-  p->kg.offset_range(side, lo, hi);
-  if (lo < INT32_MIN || hi > INT32_MAX) return QS_OK;
-  std::vector<int64_t> o((size_t)p->K);
-  p->kg.fill_offsets(side, 0, p->K, o.data());
-  std::vector<int32_t> h((size_t)((p->K + 3) & ~int64_t(3)), 0);
-  for (int64_t k = 0; k < p->K; ++k) h[(size_t)k] = (int32_t)o[(size_t)k];
-  void *q;
-  int rc = tc_alloc(p, &q, h.size() * sizeof(int32_t));
-  if (rc) return rc;
-  if (reinterpret_cast<uintptr_t>(q) & 15) return QS_OK;  // a caller allocator's odd block: int64 map
-  if (setup_upload(q, h.data(), h.size() * sizeof(int32_t)) != cudaSuccess)
-    return fail(QS_ECUDA, "cudaMemcpyAsync (int32 K offsets)");
-  p->ws.offK32[side] = (int32_t *)q;
-  return QS_OK;
-}
-
 int tc_prepare(qs_plan *p) {
   tc_geometry(p);
   const TensorCoreGeom &g = p->tc;
@@ -1837,9 +1500,10 @@ int tc_prepare(qs_plan *p) {
   p->ws.panelA = q;
   if ((rc = tc_alloc(p, &q, (size_t)g.plane_bytes_b * g.nslices))) return rc;
   p->ws.panelB = q;
-  if (p->method == QS_METHOD_OZAKI_I8)
-    for (int side = 0; side < 2; ++side)
-      if ((rc = upload_koff32(p, side))) return rc;
+  if (p->method == QS_METHOD_OZAKI_I8) {
+    if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
+    p->ws.rowmax = (unsigned long long *)q;
+  }
   if (p->method == QS_METHOD_OZAKI_I8 && oz_fixed_slices(g.nslices) &&
       !(p->opts.flags & (QS_PLAN_OZ_SINGLE_SM | QS_PLAN_PER_PRODUCT_GEMM)))
     p->oz_pair_maps = make_pair_maps(p) ? 1 : 0;  // else the one-SM kernel runs
@@ -1923,7 +1587,7 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   a.K = p->K * g.kmul;
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
-  a.offK32 = p->ws.offK32[side];
+  a.rowmax = p->ws.rowmax ? p->ws.rowmax + (side == 0 ? 0 : g.Mp) : nullptr;
   if (p->method == QS_METHOD_OZAKI_I8) {
     int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
     int32_t *counters = lists + g.Mp + g.Np;
@@ -2056,24 +1720,22 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   if (oz) {
     int32_t *counters = p->ws.expA + g.Mp + g.Np + g.Mp + g.Np;
     e = cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->ws.rowmax, 0, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(QS_ECUDA, "cudaMemsetAsync");
   }
   if (ev) cudaEventRecord(ev[0], st);
   {
-    // Both operands per launch.  Profile stages: ev[1] and ev[2] both after
-    // the pack (Ozaki: the fused row-max + digit-plane kernel).
+    // Profile stages: Ozaki: ev[1] after A's two passes, ev[2] after B's;
+    // BF16x3 (both operands per launch): both after the pack.
     const PackArgs pa = pack_args(p, 0), pb = pack_args(p, 1);
     const int nrbA = (int)cdiv(pa.rows_pad, 32), nrbB = (int)cdiv(pb.rows_pad, 32);
     const int64_t nA = (int64_t)nrbA * g.kblocks, nB = (int64_t)nrbB * g.kblocks;
     if (oz) {
-      const int64_t nbA = cdiv(pa.rows_pad, kBandRows), nbB = cdiv(pb.rows_pad, kBandRows);
-      const int grid = (int)std::min<int64_t>(nbA + nbB, kPackCtasPerSm * (int64_t)num_sms());
-      launch_pack_fused(pa, pb, nbA, nbB, grid, st);
-      if (ev) {
-        cudaEventRecord(ev[1], st);
-        cudaEventRecord(ev[2], st);
-      }
-      ++launches;
+      launch_pack_operand(pa, st);
+      if (ev) cudaEventRecord(ev[1], st);
+      launch_pack_operand(pb, st);
+      if (ev) cudaEventRecord(ev[2], st);
+      launches += 4;
     } else {
       bf16_pack_pair_kernel<<<(unsigned)(nA + nB), 256, 0, st>>>(pa, pb, nrbA, nrbB, nA);
       if (ev) {
@@ -2133,18 +1795,19 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
 // reads per-problem arguments from device tables.
 
 // One operand side of one problem in a grouped pack launch: blocks
-// [block_start, block_start + gx * kblocks) of the launch.
-// Ozaki: blocks are kBandRows-row bands (gx of them); BF16x3: 32-row x 64-K
-// blocks (gx row blocks x kblocks).
+// [block_start, block_start + gx * kblocks) of the launch, gx row blocks of
+// 32 rows by kblocks K blocks (Ozaki: 128 K values; BF16x3: 64).
 struct PackJob {
   PackArgs pa;
   int gx;
   int block_start;
 };
 
-// A per-plan prep: the non-finite counters to zero.
+// A per-plan prep: the non-finite counters and the row maxima to zero.
 struct ZeroJob {
   int32_t *counters;
+  unsigned long long *rowmax;
+  int64_t nrows;
 };
 
 __device__ __forceinline__ int pack_job(const PackJob *jobs, int njobs, int b) {
@@ -2157,30 +1820,32 @@ __device__ __forceinline__ int pack_job(const PackJob *jobs, int njobs, int b) {
   return lo;
 }
 
+// One block per plan (grid-strided).
 __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int n) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += gridDim.x * blockDim.x)
-    jobs[j >> 1].counters[j & 1] = 0;
+  for (int j = blockIdx.x; j < n; j += gridDim.x) {
+    const ZeroJob z = jobs[j];
+    if (threadIdx.x < 2) z.counters[threadIdx.x] = 0;
+    for (int64_t i = threadIdx.x; i < z.nrows; i += blockDim.x) z.rowmax[i] = 0;
+  }
 }
 
-// The fused pack over every band of every (problem, side) job.
-struct GroupBands {
-  const PackJob *jobs;
-  int njobs, nbands;
-  __device__ __forceinline__ int64_t count() const { return nbands; }
-  __device__ __forceinline__ int find(int64_t b) const { return pack_job(jobs, njobs, (int)b); }
-  __device__ __forceinline__ const PackArgs *args(int j) const { return &jobs[j].pa; }
-  __device__ __forceinline__ int64_t first(int j) const { return jobs[j].block_start; }
-  __device__ __forceinline__ int64_t last(int j) const {
-    return j + 1 < njobs ? jobs[j + 1].block_start : nbands;
-  }
-};
+// The two pack passes over every (problem, side) job: job j owns blocks
+// [block_start, block_start + gx * kblocks) of the launch (row block
+// fastest); pass 1 skips the K blocks past K.
+template <int KIND>
+__global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, int njobs) {
+  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+  const int lb = blockIdx.x - j.block_start;
+  const int64_t r0 = (int64_t)(lb % j.gx) * kPackRows, k0 = (int64_t)(lb / j.gx) * kPackK;
+  if (k0 >= j.pa.K) return;
+  oz_rowmax_block<KIND>(j.pa, r0, k0);
+}
 
 template <int KIND>
-__global__ void __launch_bounds__(kPackThreads, kPackCtasPerSm)
-    oz_pack_fused_grouped(const PackJob *jobs, int njobs, int nbands) {
-  extern __shared__ __align__(16) double pack_ring[];
-  oz_pack_walk<KIND>(GroupBands{jobs, njobs, nbands}, pack_ring,
-                     reinterpret_cast<int32_t *>(reinterpret_cast<uint8_t *>(pack_ring) + kPackRingBytes));
+__global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, int njobs) {
+  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+  const int lb = blockIdx.x - j.block_start;
+  oz_digit_block<KIND>(j.pa, (int64_t)(lb % j.gx) * kPackRows, (int64_t)(lb / j.gx) * kPackK);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
@@ -2227,9 +1892,9 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
     for (int side = 0; side < 2; ++side) {
       PackJob j;
       j.pa = pack_args(p, side);
-      j.gx = (int)cdiv(j.pa.rows_pad, oz ? kBandRows : 32);
+      j.gx = (int)cdiv(j.pa.rows_pad, 32);
       j.block_start = blocks;
-      const int64_t nb = oz ? (int64_t)j.gx : (int64_t)j.gx * tg.kblocks;
+      const int64_t nb = (int64_t)j.gx * tg.kblocks;
       if (blocks + nb > INT_MAX) return fail(QS_EINVAL, "ArgumentError: grouped pack launch too large");
       blocks += (int)nb;
       jobs.push_back(j);
@@ -2241,6 +1906,8 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
     if (oz) {
       ZeroJob z;
       z.counters = p->ws.expA + tg.Mp + tg.Np + tg.Mp + tg.Np;
+      z.rowmax = p->ws.rowmax;
+      z.nrows = tg.Mp + tg.Np;
       zero.push_back(z);
       fix.push_back(make_fixup_job(p, al, be, bcase[g.idx[i]]));
     }
@@ -2254,7 +1921,6 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
       if (pack_kind_of(j.pa) != g.pack_kind) g.pack_kind = kPackAny;
   }
   g.tiles = tiles.back();
-  if (oz && blocks > 0) g.pack_grid = (int)std::min<int64_t>(blocks, (int64_t)kPackCtasPerSm * num_sms());
   size_t off = 0;
   g.off_pack = off;
   off = align_up(off + jobs.size() * sizeof(PackJob), 64);
@@ -2317,23 +1983,22 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const ZeroJob *zero = (const ZeroJob *)(d + g.off_zero);
     const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
     const int pgrid = std::min(n, 4 * num_sms());
-    oz_prep_grouped<<<(unsigned)cdiv(2 * n, 256), 256, 0, st>>>(zero, n);
-    static std::atomic<int> done[3];
-    const int pgrid2 = g.pack_grid;
-    switch (pgrid2 > 0 ? g.pack_kind : -1) {
+    oz_prep_grouped<<<(unsigned)std::min(n, 4 * num_sms()), 256, 0, st>>>(zero, n);
+    const unsigned pb = (unsigned)g.pack_blocks;
+    switch (pb > 0 ? g.pack_kind : -1) {
       case -1:
         break;
       case kPackF64:
-        pack_smem_attr(oz_pack_fused_grouped<kPackF64>, done[0]);
-        oz_pack_fused_grouped<kPackF64><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_rowmax_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_digit_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, g.njobs);
         break;
       case kPackF32:
-        pack_smem_attr(oz_pack_fused_grouped<kPackF32>, done[1]);
-        oz_pack_fused_grouped<kPackF32><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_rowmax_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_digit_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, g.njobs);
         break;
       default:
-        pack_smem_attr(oz_pack_fused_grouped<kPackAny>, done[2]);
-        oz_pack_fused_grouped<kPackAny><<<pgrid2, kPackThreads, kPackSmem, st>>>(jobs, g.njobs, g.pack_blocks);
+        oz_rowmax_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_digit_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, g.njobs);
         break;
     }
     if (g.cls == TC_CLASS_OZ4)
@@ -2345,7 +2010,7 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     else
       tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(base, gt);
     oz_fixup_grouped<<<pgrid, 256, 0, st>>>(fix, n);
-    l = 4;  // prep, fused pack, GEMM, fixup
+    l = 5;  // prep, row maxima, digits, GEMM, fixup
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -36,7 +36,6 @@ struct TcGroup {
   size_t dev_bytes = 0;
   size_t off_pack = 0, off_gemm = 0, off_tiles = 0, off_zero = 0, off_fix = 0;
   int njobs = 0, pack_blocks = 0, tiles = 0;
-  int pack_grid = 0;  // CTAs of the fused pack launch
   int pack_kind = 2;  // element kind of the fused pack walk (tc.cu kPack*)
 };
 // alpha/beta hold 2 doubles per plan of the group, bcase one int per plan.
