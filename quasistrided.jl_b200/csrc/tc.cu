@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <climits>
 #include <cstdlib>
@@ -645,6 +646,7 @@ __device__ __forceinline__ int64_t c_col(const GemmArgs &a, int64_t n) {
 struct GemmTable {
   const GemmArgs *tab;
   const int *tile_start;
+  const int *tile_prob;  // problem of each tile of the launch
   int nprob;
 };
 
@@ -655,14 +657,9 @@ __device__ __forceinline__ const GemmArgs &tile_problem(const GemmArgs &a, const
     local = t;
     return a;
   }
-  int lo = 0, hi = g.nprob - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(g.tile_start + mid) <= t) lo = mid;
-    else hi = mid - 1;
-  }
-  local = t - __ldg(g.tile_start + lo);
-  return g.tab[lo];
+  const int p = __ldg(g.tile_prob + t);
+  local = t - __ldg(g.tile_start + p);
+  return g.tab[p];
 }
 
 // Segments of a tile: Ozaki, one per (diagonal, K segment); BF16x3, one per
@@ -1750,24 +1747,24 @@ int tc_execute(qs_plan *p, const double *alpha, const double *beta, int beta_cas
   const int grid = std::min(tiles, num_sms());
   if (oz) {
     if (p->opts.flags & QS_PLAN_PER_PRODUCT_GEMM) {
-      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
     } else if (oz_fixed_slices(g.nslices) && p->oz_pair_maps) {
       e = launch_oz_pair(g.nslices, a, p->oz_tmap, st);
       if (e != cudaSuccess) return fail(QS_ECUDA, std::string("CTA-pair GEMM launch: ") + cudaGetErrorString(e));
     } else if (g.nslices == 4) {
-      oz_gemm_fixed_kernel<4, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+      oz_gemm_fixed_kernel<4, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
     } else if (g.nslices == 6) {
-      oz_gemm_fixed_kernel<6, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+      oz_gemm_fixed_kernel<6, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
     } else if (g.nslices == 7) {
-      oz_gemm_fixed_kernel<7, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+      oz_gemm_fixed_kernel<7, false><<<grid, 320, oz_smem_bytes(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
     } else if (g.nslices <= 8) {
       const OzSched sched = build_oz_sched(g.nslices);
       oz_gemm_kernel<<<grid, 320, oz_smem_bytes(), st>>>(a, sched);
     } else {
-      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+      tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
     }
   } else {
-    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a, GemmTable{nullptr, nullptr, 0});
+    tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(a, GemmTable{nullptr, nullptr, nullptr, 0});
   }
   ++launches;
   if (ev) cudaEventRecord(ev[3], st);
@@ -1810,16 +1807,6 @@ struct ZeroJob {
   int64_t nrows;
 };
 
-__device__ __forceinline__ int pack_job(const PackJob *jobs, int njobs, int b) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].block_start <= b) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 // One block per plan (grid-strided).
 __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int n) {
   for (int j = blockIdx.x; j < n; j += gridDim.x) {
@@ -1831,10 +1818,10 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
 
 // The two pack passes over every (problem, side) job: job j owns blocks
 // [block_start, block_start + gx * kblocks) of the launch (row block
-// fastest); pass 1 skips the K blocks past K.
+// fastest), jobmap[b] the job of block b; pass 1 skips the K blocks past K.
 template <int KIND>
-__global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, int njobs) {
-  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+__global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, const int *jobmap) {
+  const PackJob &j = jobs[__ldg(jobmap + blockIdx.x)];
   const int lb = blockIdx.x - j.block_start;
   const int64_t r0 = (int64_t)(lb % j.gx) * kPackRows, k0 = (int64_t)(lb / j.gx) * kPackK;
   if (k0 >= j.pa.K) return;
@@ -1842,14 +1829,14 @@ __global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs,
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, int njobs) {
-  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+__global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, const int *jobmap) {
+  const PackJob &j = jobs[__ldg(jobmap + blockIdx.x)];
   const int lb = blockIdx.x - j.block_start;
   oz_digit_block<KIND>(j.pa, (int64_t)(lb % j.gx) * kPackRows, (int64_t)(lb / j.gx) * kPackK);
 }
 
-__global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, int njobs) {
-  const PackJob &j = jobs[pack_job(jobs, njobs, blockIdx.x)];
+__global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, const int *jobmap) {
+  const PackJob &j = jobs[__ldg(jobmap + blockIdx.x)];
   const int lb = blockIdx.x - j.block_start;
   const PackArgs pa = j.pa;
   bf16_pack_block(pa, (int64_t)(lb % j.gx) * 32, (int64_t)(lb / j.gx) * 64);
@@ -1914,6 +1901,11 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   }
   g.njobs = (int)jobs.size();
   g.pack_blocks = blocks;
+  std::vector<int> jobmap((size_t)blocks);
+  for (size_t jj = 0; jj < jobs.size(); ++jj) {
+    const int end = jj + 1 < jobs.size() ? jobs[jj + 1].block_start : blocks;
+    std::fill(jobmap.begin() + jobs[jj].block_start, jobmap.begin() + end, (int)jj);
+  }
   g.pack_kind = kPackAny;
   if (oz && !jobs.empty()) {
     g.pack_kind = pack_kind_of(jobs[0].pa);
@@ -1921,6 +1913,8 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
       if (pack_kind_of(j.pa) != g.pack_kind) g.pack_kind = kPackAny;
   }
   g.tiles = tiles.back();
+  std::vector<int> tilemap((size_t)g.tiles);
+  for (int i = 0; i < n; ++i) std::fill(tilemap.begin() + tiles[i], tilemap.begin() + tiles[i + 1], i);
   size_t off = 0;
   g.off_pack = off;
   off = align_up(off + jobs.size() * sizeof(PackJob), 64);
@@ -1932,6 +1926,10 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   off = align_up(off + zero.size() * sizeof(ZeroJob), 64);
   g.off_fix = off;
   off = align_up(off + fix.size() * sizeof(FixupJob), 64);
+  g.off_jobmap = off;
+  off = align_up(off + jobmap.size() * sizeof(int), 64);
+  g.off_tilemap = off;
+  off = align_up(off + tilemap.size() * sizeof(int), 64);
   g.image.assign(off, 0);
   auto put = [&](size_t at, const void *src, size_t bytes) {
     if (bytes) std::memcpy(g.image.data() + at, src, bytes);
@@ -1941,6 +1939,8 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   put(g.off_tiles, tiles.data(), tiles.size() * sizeof(int));
   put(g.off_zero, zero.data(), zero.size() * sizeof(ZeroJob));
   put(g.off_fix, fix.data(), fix.size() * sizeof(FixupJob));
+  put(g.off_jobmap, jobmap.data(), jobmap.size() * sizeof(int));
+  put(g.off_tilemap, tilemap.data(), tilemap.size() * sizeof(int));
   return QS_OK;
 }
 
@@ -1968,7 +1968,7 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
   const PackJob *jobs = (const PackJob *)(d + g.off_pack);
   const GemmArgs *tab = (const GemmArgs *)(d + g.off_gemm);
   const int *tile_start = (const int *)(d + g.off_tiles);
-  const GemmTable gt{tab, tile_start, n};
+  const GemmTable gt{tab, tile_start, (const int *)(d + g.off_tilemap), n};
   // The kernel's own GemmArgs: the first problem's (the launch-wide status
   // word and the table-independent fields).
   GemmArgs base;
@@ -1976,7 +1976,7 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
   const int grid = std::min(g.tiles, num_sms());
   int l = 0;
   if (g.cls == TC_CLASS_BF16) {
-    bf16_pack_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, g.njobs);
+    bf16_pack_grouped<<<g.pack_blocks, 256, 0, st>>>(jobs, (const int *)(d + g.off_jobmap));
     tc_gemm_kernel<KIND_BF16><<<grid, 192, gemm_smem_bytes<KIND_BF16>(), st>>>(base, gt);
     l = 2;
   } else {
@@ -1985,20 +1985,21 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const int pgrid = std::min(n, 4 * num_sms());
     oz_prep_grouped<<<(unsigned)std::min(n, 4 * num_sms()), 256, 0, st>>>(zero, n);
     const unsigned pb = (unsigned)g.pack_blocks;
+    const int *jobmap = (const int *)(d + g.off_jobmap);
     switch (pb > 0 ? g.pack_kind : -1) {
       case -1:
         break;
       case kPackF64:
-        oz_rowmax_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, g.njobs);
-        oz_digit_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_rowmax_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, jobmap);
+        oz_digit_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, jobmap);
         break;
       case kPackF32:
-        oz_rowmax_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, g.njobs);
-        oz_digit_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_rowmax_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, jobmap);
+        oz_digit_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, jobmap);
         break;
       default:
-        oz_rowmax_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, g.njobs);
-        oz_digit_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, g.njobs);
+        oz_rowmax_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, jobmap);
+        oz_digit_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, jobmap);
         break;
     }
     if (g.cls == TC_CLASS_OZ4)

@@ -34,7 +34,7 @@ struct TcGroup {
   std::vector<uint8_t> image;
   void *dev = nullptr;
   size_t dev_bytes = 0;
-  size_t off_pack = 0, off_gemm = 0, off_tiles = 0, off_zero = 0, off_fix = 0;
+  size_t off_pack = 0, off_gemm = 0, off_tiles = 0, off_zero = 0, off_fix = 0, off_jobmap = 0, off_tilemap = 0;
   int njobs = 0, pack_blocks = 0, tiles = 0;
   int pack_kind = 2;  // element kind of the fused pack walk (tc.cu kPack*)
 };
