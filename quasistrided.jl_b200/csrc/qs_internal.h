@@ -84,6 +84,7 @@ struct Workspace {
   int32_t *expA = nullptr;  // per packed row of A (Ozaki), or nullptr
   int32_t *expB = nullptr;
   unsigned long long *rowmax = nullptr;  // Ozaki: row maxima of A (Mp) then B (Np)
+  int32_t *rperm[2] = {nullptr, nullptr};  // Ozaki pack row orders (A, B), or nullptr
   int32_t *status = nullptr;  // device status word (bounded waits)
   size_t bytes = 0;
   std::vector<void *> owned;         // every allocated block, for freeing

@@ -78,7 +78,17 @@ struct PackArgs {
   // Ozaki pass 1 -> pass 2: each padded row's max |x| bit pattern (zeroed
   // before every pack), or nullptr.
   unsigned long long *rowmax;
+  // The order in which the pack visits rows (rows_pad entries: tile row i
+  // is virtual row rperm[i]), or nullptr for 0, 1, 2, ...  A real operand
+  // whose unit-stride axis is a later label of its row group gets the order
+  // with that label fastest, so a warp's 32 rows are adjacent in memory.
+  const int32_t *rperm;
 };
+
+// Virtual row of the pack's row position i.
+__device__ __forceinline__ int64_t pack_row(const PackArgs &a, int64_t i) {
+  return a.rperm ? (int64_t)__ldg(a.rperm + i) : i;
+}
 
 // Element (r, k) of the real (virtual) matrix the panels hold.
 template <class T>
@@ -122,7 +132,7 @@ __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, in
   const S *X = static_cast<const S *>(a.X) + a.Xbase;
   if (a.rfast) {
     const int rr = tid & 31, kb = tid >> 5;
-    const int64_t r = r0 + rr;
+    const int64_t r = pack_row(a, r0 + rr);
     const bool rok = r < a.rows;
     const int64_t ro = rok ? __ldg(a.offR + r) : 0;
 #pragma unroll
@@ -142,7 +152,7 @@ __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, in
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int rr = rb + RSTEP * i;
-      const int64_t r = r0 + rr;
+      const int64_t r = pack_row(a, r0 + rr);
       const bool ok = kok && r < a.rows;
       const int64_t ro = ok ? __ldg(a.offR + r) : 0;
       tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
@@ -162,7 +172,7 @@ __device__ __forceinline__ void load_tile(const PackArgs &a, int64_t r0, int64_t
   for (int i = 0; i < PER; ++i) {
     int e = tid + 256 * i, rr, kk;
     if (a.rfast) { rr = e & 31; kk = e >> 5; } else { kk = e % KT; rr = e / KT; }
-    int64_t r = r0 + rr, k = k0 + kk;
+    int64_t r = pack_row(a, r0 + rr), k = k0 + kk;
     T v = (T)0;
     if (r < a.rows && k < a.K) v = virtual_elem<T>(a, r, k);
     tile[rr][tcol<KT>(kk)] = v;
@@ -277,7 +287,8 @@ __device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, int64_t r0, i
     const unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
     m = x > m ? x : m;
   }
-  if (part == 0 && r0 + row < a.rows && m) atomicMax(a.rowmax + r0 + row, m);
+  const int64_t r = pack_row(a, r0 + row);
+  if (part == 0 && r < a.rows && m) atomicMax(a.rowmax + r, m);
 }
 
 // The row's exponent E (frexp exponent of the max + 1; kNonFinite for a row
@@ -312,7 +323,7 @@ __device__ __forceinline__ void oz_digit_block(const PackArgs &a, int64_t r0, in
   pack_load<KIND>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, c = threadIdx.x & 7;
-  const int64_t grow = r0 + row;
+  const int64_t grow = pack_row(a, r0 + row);
   if (grow >= a.rows_pad) return;
   const int s = a.nslices;
   const RowScale rs = row_scale(grow < a.rows ? __ldg(a.rowmax + grow) : 0ull, s);
@@ -1488,6 +1499,57 @@ static bool make_pair_maps(qs_plan *p) {
   return true;
 }
 
+// The pack's row order for a real operand (side 0: A over M, 1: B over N)
+// whose unit-stride axis is neither the first label of its row group nor
+// the first K label but a later row label d*: rows enumerated with d*
+// fastest, then the others in order (row index r = sum_d x_d R_d, first
+// label fastest).  Padding rows keep their place.  Else no table.
+static int upload_row_order(qs_plan *p, int side) {
+  const TensorCoreGeom &g = p->tc;
+  const Group &G = side == 0 ? p->mg : p->ng;
+  const int T = side == 0 ? p->TA : p->TB;
+  if (g.cplx_layout != 0 || is_complex(T) || G.D < 2) return QS_OK;
+  auto unit = [](int64_t st, int64_t len) { return len > 1 && (st == 1 || st == -1); };
+  if (unit(G.st[0][0], G.len[0])) return QS_OK;                        // rows already unit-stride
+  if (p->kg.D > 0 && unit(p->kg.st[side][0], p->kg.len[0])) return QS_OK;  // K-fast gather
+  int ds = -1;
+  for (int d = 1; d < G.D && ds < 0; ++d)
+    if (unit(G.st[0][d], G.len[d])) ds = d;
+  if (ds < 0) return QS_OK;
+  const int64_t rows = G.length(), rows_pad = side == 0 ? g.Mp : g.Np;
+  if (rows <= 0 || rows_pad > INT32_MAX) return QS_OK;
+  int64_t R[kMaxRank];
+  int64_t acc = 1;
+  for (int d = 0; d < G.D; ++d) {
+    R[d] = acc;
+    acc *= G.len[d];
+  }
+  int order[kMaxRank], n = 0;
+  order[n++] = ds;
+  for (int d = 0; d < G.D; ++d)
+    if (d != ds) order[n++] = d;
+  std::vector<int32_t> h((size_t)rows_pad);
+  int64_t x[kMaxRank] = {};
+  for (int64_t i = 0; i < rows; ++i) {
+    int64_t r = 0;
+    for (int d = 0; d < G.D; ++d) r += x[d] * R[d];
+    h[(size_t)i] = (int32_t)r;
+    for (int q = 0; q < n; ++q) {  // next coordinate, order[0] fastest
+      const int d = order[q];
+      if (++x[d] < G.len[d]) break;
+      x[d] = 0;
+    }
+  }
+  for (int64_t i = rows; i < rows_pad; ++i) h[(size_t)i] = (int32_t)i;
+  void *q;
+  int rc = tc_alloc(p, &q, h.size() * sizeof(int32_t));
+  if (rc) return rc;
+  if (setup_upload(q, h.data(), h.size() * sizeof(int32_t)) != cudaSuccess)
+    return fail(QS_ECUDA, "cudaMemcpyAsync (pack row order)");
+  p->ws.rperm[side] = (int32_t *)q;
+  return QS_OK;
+}
+
 int tc_prepare(qs_plan *p) {
   tc_geometry(p);
   const TensorCoreGeom &g = p->tc;
@@ -1500,6 +1562,8 @@ int tc_prepare(qs_plan *p) {
   if (p->method == QS_METHOD_OZAKI_I8) {
     if ((rc = tc_alloc(p, &q, (size_t)(g.Mp + g.Np) * sizeof(unsigned long long)))) return rc;
     p->ws.rowmax = (unsigned long long *)q;
+    for (int side = 0; side < 2; ++side)
+      if ((rc = upload_row_order(p, side))) return rc;
   }
   if (p->method == QS_METHOD_OZAKI_I8 && oz_fixed_slices(g.nslices) &&
       !(p->opts.flags & (QS_PLAN_OZ_SINGLE_SM | QS_PLAN_PER_PRODUCT_GEMM)))
@@ -1585,6 +1649,8 @@ static PackArgs pack_args(const qs_plan *p, int side) {
   a.kblocks = (int)g.kblocks;
   a.nslices = g.nslices;
   a.rowmax = p->ws.rowmax ? p->ws.rowmax + (side == 0 ? 0 : g.Mp) : nullptr;
+  a.rperm = p->ws.rperm[side];
+  if (a.rperm) a.rfast = 1;
   if (p->method == QS_METHOD_OZAKI_I8) {
     int32_t *lists = p->ws.expA + g.Mp + g.Np;  // [rows: Mp][cols: Np][2 counters]
     int32_t *counters = lists + g.Mp + g.Np;

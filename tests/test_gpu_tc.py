@@ -74,6 +74,24 @@ def test_ozaki_permuted_4index(qs, orc, wide):
     assert rel_fro(got, ref) <= TOL64, rel_fro(got, ref)
 
 
+@pytest.mark.parametrize("et,tol", [("Float64", TOL64), ("Float32", TOL32)])
+def test_ozaki_unit_stride_on_a_later_row_label(qs, orc, et, tol):
+    # C[x,y,n1,n2] = sum_k A[y,k,x] B[n2,k,n1]: the M labels are (x, y) and
+    # the N labels (n1, n2) in C's order, K is k; A is unit-stride along y
+    # and B along n2, neither along its first row label nor along K, so the
+    # pack visits their rows in the order with that label fastest.  Both
+    # operands scaled by 2^U along a row label to vary the row exponents.
+    rng = np.random.default_rng(17)
+    x, y, k, n1, n2 = 24, 40, 150, 20, 16
+    A = uniform_pair(qs, rng, (y, k, x), et, scale_axis=2)
+    B = uniform_pair(qs, rng, (n2, k, n1), et, scale_axis=0)
+    C = colmajor_pair(qs, rng, (x, y, n1, n2), et)
+    got, ref, plan = run_pair(qs, orc, C, 1.3, A, (2, 5, 1), B, (4, 5, 3), 0.7, (1, 2, 3, 4),
+                              method="ozaki", precision=1)
+    assert plan.method == "ozaki" and plan.m_labels == (1, 2) and plan.n_labels == (3, 4)
+    assert rel_fro(got, ref) <= tol, rel_fro(got, ref)
+
+
 def test_ozaki_persistent_tiles_and_reuse(qs, orc):
     # 16 x 16 = 256 tiles > SM count: every CTA runs more than one tile.
     rng = np.random.default_rng(9)
