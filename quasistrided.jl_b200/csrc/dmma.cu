@@ -278,7 +278,7 @@ struct DmmaShape<2> { using Cfg = DmmaCfg<64, 64, 2, 2, 4>; };
 template <>
 struct DmmaShape<3> { using Cfg = DmmaCfg<128, 32, 8, 1, 4>; };
 template <>
-struct DmmaShape<4> { using Cfg = DmmaCfg<256, 16, 8, 1, 4>; };
+struct DmmaShape<4> { using Cfg = DmmaCfg<256, 16, 8, 1, 3>; };  // 104 KB: two CTAs per SM
 template <>
 struct DmmaShape<5> { using Cfg = DmmaCfg<128, 128, 4, 4, 4>; };
 

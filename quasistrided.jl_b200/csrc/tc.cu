@@ -246,6 +246,8 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 // passes operand by operand, so the second pass re-reads an operand that
 // the first has just brought into L2.
 constexpr int kPackRows = 32, kPackK = 128;
+// Operand bytes per chunk of a grouped pack (pass 2 re-reads them from L2).
+constexpr size_t kPackChunkBytes = 64ull << 20;
 
 // Element kinds, fixed per launch: real Float64 or real Float32 operands
 // take the straight-line loads of load_tile_real; anything else (complex
@@ -1882,22 +1884,27 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
   }
 }
 
-// The two pack passes over every (problem, side) job: job j owns blocks
-// [block_start, block_start + gx * kblocks) of the launch (row block
-// fastest), jobmap[b] the job of block b; pass 1 skips the K blocks past K.
+// The two pack passes over a chunk of (problem, side) jobs: job j owns
+// blocks [block_start, block_start + gx * kblocks) of the group (row block
+// fastest), jobmap[b] the job of block b, and a launch covers the chunk's
+// blocks from b0; pass 1 skips the K blocks past K.  A group packs chunk by
+// chunk (pass 1, pass 2, next chunk), each chunk's operands small enough
+// that pass 2 re-reads them from L2.
 template <int KIND>
-__global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, const int *jobmap) {
-  const PackJob &j = jobs[__ldg(jobmap + blockIdx.x)];
-  const int lb = blockIdx.x - j.block_start;
+__global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, const int *jobmap, int b0) {
+  const int b = b0 + (int)blockIdx.x;
+  const PackJob &j = jobs[__ldg(jobmap + b)];
+  const int lb = b - j.block_start;
   const int64_t r0 = (int64_t)(lb % j.gx) * kPackRows, k0 = (int64_t)(lb / j.gx) * kPackK;
   if (k0 >= j.pa.K) return;
   oz_rowmax_block<KIND>(j.pa, r0, k0);
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, const int *jobmap) {
-  const PackJob &j = jobs[__ldg(jobmap + blockIdx.x)];
-  const int lb = blockIdx.x - j.block_start;
+__global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, const int *jobmap, int b0) {
+  const int b = b0 + (int)blockIdx.x;
+  const PackJob &j = jobs[__ldg(jobmap + b)];
+  const int lb = b - j.block_start;
   oz_digit_block<KIND>(j.pa, (int64_t)(lb % j.gx) * kPackRows, (int64_t)(lb / j.gx) * kPackK);
 }
 
@@ -1967,6 +1974,23 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
   }
   g.njobs = (int)jobs.size();
   g.pack_blocks = blocks;
+  // Pack chunks: consecutive jobs up to kPackChunkBytes of operand data
+  // (a job larger than that is a chunk of its own).
+  g.chunks.assign(1, 0);
+  {
+    size_t bytes = 0;
+    for (size_t jj = 0; jj < jobs.size(); ++jj) {
+      const PackArgs &pa = jobs[jj].pa;
+      const size_t jb = (size_t)pa.rows * (size_t)pa.K * 8;  // about: 8 bytes per virtual element
+      if (bytes > 0 && bytes + jb > kPackChunkBytes) {
+        g.chunks.push_back(jobs[jj].block_start);
+        bytes = 0;
+      }
+      bytes += jb;
+    }
+    if (blocks > 0) g.chunks.push_back(blocks);
+    else g.chunks.clear();
+  }
   std::vector<int> jobmap((size_t)blocks);
   for (size_t jj = 0; jj < jobs.size(); ++jj) {
     const int end = jj + 1 < jobs.size() ? jobs[jj + 1].block_start : blocks;
@@ -2050,23 +2074,24 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const FixupJob *fix = (const FixupJob *)(d + g.off_fix);
     const int pgrid = std::min(n, 4 * num_sms());
     oz_prep_grouped<<<(unsigned)std::min(n, 4 * num_sms()), 256, 0, st>>>(zero, n);
-    const unsigned pb = (unsigned)g.pack_blocks;
     const int *jobmap = (const int *)(d + g.off_jobmap);
-    switch (pb > 0 ? g.pack_kind : -1) {
-      case -1:
-        break;
-      case kPackF64:
-        oz_rowmax_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, jobmap);
-        oz_digit_grouped<kPackF64><<<pb, 256, 0, st>>>(jobs, jobmap);
-        break;
-      case kPackF32:
-        oz_rowmax_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, jobmap);
-        oz_digit_grouped<kPackF32><<<pb, 256, 0, st>>>(jobs, jobmap);
-        break;
-      default:
-        oz_rowmax_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, jobmap);
-        oz_digit_grouped<kPackAny><<<pb, 256, 0, st>>>(jobs, jobmap);
-        break;
+    for (size_t c = 0; c + 1 < g.chunks.size(); ++c) {
+      const int b0 = g.chunks[c];
+      const unsigned nb = (unsigned)(g.chunks[c + 1] - b0);
+      switch (g.pack_kind) {
+        case kPackF64:
+          oz_rowmax_grouped<kPackF64><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          oz_digit_grouped<kPackF64><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          break;
+        case kPackF32:
+          oz_rowmax_grouped<kPackF32><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          oz_digit_grouped<kPackF32><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          break;
+        default:
+          oz_rowmax_grouped<kPackAny><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          oz_digit_grouped<kPackAny><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
+          break;
+      }
     }
     if (g.cls == TC_CLASS_OZ4)
       oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
@@ -2077,7 +2102,7 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     else
       tc_gemm_kernel<KIND_I8><<<grid, 192, gemm_smem_bytes<KIND_I8>(), st>>>(base, gt);
     oz_fixup_grouped<<<pgrid, 256, 0, st>>>(fix, n);
-    l = 5;  // prep, row maxima, digits, GEMM, fixup
+    l = 3 + 2 * ((int)g.chunks.size() - 1);  // prep, per chunk row maxima + digits, GEMM, fixup
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -36,7 +36,8 @@ struct TcGroup {
   size_t dev_bytes = 0;
   size_t off_pack = 0, off_gemm = 0, off_tiles = 0, off_zero = 0, off_fix = 0, off_jobmap = 0, off_tilemap = 0;
   int njobs = 0, pack_blocks = 0, tiles = 0;
-  int pack_kind = 2;  // element kind of the fused pack walk (tc.cu kPack*)
+  int pack_kind = 2;       // element kind of the pack passes (tc.cu kPack*)
+  std::vector<int> chunks;  // Ozaki pack chunks: block boundaries, first 0, last pack_blocks
 };
 // alpha/beta hold 2 doubles per plan of the group, bcase one int per plan.
 int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const int *bcase);
