@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 // the first has just brought into L2.
 constexpr int kPackRows = 32, kPackK = 128;
 // Operand bytes per chunk of a grouped pack (pass 2 re-reads them from L2).
-constexpr size_t kPackChunkBytes = 64ull << 20;
+constexpr size_t kPackChunkBytes = 48ull << 20;
 
 // Element kinds, fixed per launch: real Float64 or real Float32 operands
 // take the straight-line loads of load_tile_real; anything else (complex
@@ -2039,6 +2039,18 @@ int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const in
 // building and dropping groups never synchronizes the device.
 int tc_group_upload(TcGroup &g, cudaStream_t st) {
   if (g.dev) return fail(QS_EINVAL, "internal: grouped tables already uploaded");
+  const int nchunks = (int)g.chunks.size() - 1;
+  if (nchunks > 0) {
+    cudaError_t e0 = cudaSuccess;
+    if (!g.aux) e0 = cudaStreamCreateWithFlags(&g.aux, cudaStreamNonBlocking);
+    while (e0 == cudaSuccess && (int)g.ev.size() < nchunks) {
+      cudaEvent_t ev;
+      e0 = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e0 == cudaSuccess) g.ev.push_back(ev);
+    }
+    if (e0 == cudaSuccess && !g.join) e0 = cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming);
+    if (e0 != cudaSuccess) return fail(QS_ECUDA, std::string("grouped pack streams: ") + cudaGetErrorString(e0));
+  }
   cudaError_t e = cudaMallocAsync(&g.dev, g.image.size(), st);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -2075,23 +2087,30 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
     const int pgrid = std::min(n, 4 * num_sms());
     oz_prep_grouped<<<(unsigned)std::min(n, 4 * num_sms()), 256, 0, st>>>(zero, n);
     const int *jobmap = (const int *)(d + g.off_jobmap);
-    for (size_t c = 0; c + 1 < g.chunks.size(); ++c) {
+    // Row maxima chunk by chunk on st; each chunk's digits on the aux stream
+    // after it, so the row maxima of chunk c + 1 overlap the digits of c.
+    const int nchunks = (int)g.chunks.size() - 1;
+    if (nchunks > 0 && (!g.aux || (int)g.ev.size() < nchunks || !g.join))
+      return fail(QS_EINVAL, "internal: grouped pack streams not created");
+    for (int c = 0; c < nchunks; ++c) {
       const int b0 = g.chunks[c];
       const unsigned nb = (unsigned)(g.chunks[c + 1] - b0);
       switch (g.pack_kind) {
-        case kPackF64:
-          oz_rowmax_grouped<kPackF64><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          oz_digit_grouped<kPackF64><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          break;
-        case kPackF32:
-          oz_rowmax_grouped<kPackF32><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          oz_digit_grouped<kPackF32><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          break;
-        default:
-          oz_rowmax_grouped<kPackAny><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          oz_digit_grouped<kPackAny><<<nb, 256, 0, st>>>(jobs, jobmap, b0);
-          break;
+        case kPackF64: oz_rowmax_grouped<kPackF64><<<nb, 256, 0, st>>>(jobs, jobmap, b0); break;
+        case kPackF32: oz_rowmax_grouped<kPackF32><<<nb, 256, 0, st>>>(jobs, jobmap, b0); break;
+        default: oz_rowmax_grouped<kPackAny><<<nb, 256, 0, st>>>(jobs, jobmap, b0); break;
       }
+      cudaEventRecord(g.ev[c], st);
+      cudaStreamWaitEvent(g.aux, g.ev[c], 0);
+      switch (g.pack_kind) {
+        case kPackF64: oz_digit_grouped<kPackF64><<<nb, 256, 0, g.aux>>>(jobs, jobmap, b0); break;
+        case kPackF32: oz_digit_grouped<kPackF32><<<nb, 256, 0, g.aux>>>(jobs, jobmap, b0); break;
+        default: oz_digit_grouped<kPackAny><<<nb, 256, 0, g.aux>>>(jobs, jobmap, b0); break;
+      }
+    }
+    if (nchunks > 0) {
+      cudaEventRecord(g.join, g.aux);
+      cudaStreamWaitEvent(st, g.join, 0);
     }
     if (g.cls == TC_CLASS_OZ4)
       oz_gemm_fixed_kernel<4, true><<<grid, 320, oz_smem_bytes(), st>>>(base, gt);
@@ -2116,6 +2135,14 @@ int tc_group_launch(const TcGroup &g, cudaStream_t st, int *launches) {
 }
 
 void tc_group_release(TcGroup &g, cudaStream_t rel) {
+  // Events and the aux stream go once their pending work is done (the
+  // runtime defers the release); the tables after their last use on rel.
+  for (cudaEvent_t e : g.ev) cudaEventDestroy(e);
+  g.ev.clear();
+  if (g.join) cudaEventDestroy(g.join);
+  g.join = nullptr;
+  if (g.aux) cudaStreamDestroy(g.aux);
+  g.aux = nullptr;
   if (g.dev) cudaFreeAsync(g.dev, rel);
   g.dev = nullptr;
   g.dev_bytes = 0;

@@ -38,6 +38,11 @@ struct TcGroup {
   int njobs = 0, pack_blocks = 0, tiles = 0;
   int pack_kind = 2;       // element kind of the pack passes (tc.cu kPack*)
   std::vector<int> chunks;  // Ozaki pack chunks: block boundaries, first 0, last pack_blocks
+  // Ozaki: the digit passes run on `aux`, chunk c after its row maxima
+  // (event ev[c] on the launch stream), joined back through `join`.
+  cudaStream_t aux = nullptr;
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t join = nullptr;
 };
 // alpha/beta hold 2 doubles per plan of the group, bcase one int per plan.
 int tc_group_build(TcGroup &g, const double *alpha, const double *beta, const int *bcase);
