@@ -246,8 +246,10 @@ __global__ void __launch_bounds__(256) bf16_pack_pair_kernel(PackArgs pa, PackAr
 // passes operand by operand, so the second pass re-reads an operand that
 // the first has just brought into L2.
 constexpr int kPackRows = 32, kPackK = 128;
-// Operand bytes per chunk of a grouped pack (pass 2 re-reads them from L2).
-constexpr size_t kPackChunkBytes = 48ull << 20;
+// Operand bytes per chunk of a grouped pack (pass 2 re-reads them from L2;
+// on the 2000-block network step 48 to 160 MB measured the same, 24 MB and
+// one chunk for the whole group 7 % slower).
+constexpr size_t kPackChunkBytes = 96ull << 20;
 
 // Element kinds, fixed per launch: real Float64 or real Float32 operands
 // take the straight-line loads of load_tile_real; anything else (complex
