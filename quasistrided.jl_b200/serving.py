@@ -9,10 +9,16 @@ Requests of mixed shapes and eltypes arrive over time.  Each loop iteration
    HBM budget and a tick slot is free (requests that arrive while others are
    on the GPU are admitted as soon as slots and memory free up);
 3. launches the admitted requests as one tick on its own stream: host->device
-   copies, plans (reused from a cache and re-pointed with ``rebind``, so the
-   steady state allocates no plan workspace), one grouped execute over all of
-   them (``ContractGroup``: one launch per stage and kernel class), and the
-   device->host copies of the results.
+   copies, one grouped execute over all of them (``ContractGroup``: one
+   launch per stage and kernel class), and the device->host copies of the
+   results.
+
+Host preparation is off that loop: with a backend that has ``prepare``, a
+preparation thread stages each request as it arrives (device blocks, pinned
+copies of host operands, its plan: reused from a cache and re-pointed with
+``rebind``, so the steady state allocates no plan workspace), after charging
+its bytes to the budget; the loop admits prepared requests only, in arrival
+order.
 
 Several ticks are in flight at once, so their work overlaps on the device.
 Operands registered with ``put_resident`` stay on the device across requests
@@ -63,6 +69,9 @@ class ContractRequest:
     result: Optional[np.ndarray] = None
     error: Optional[str] = None
     _release: Any = None
+    _prep: Any = None      # the backend's staged buffers and plan, once prepared
+    prepared: bool = False
+    _reserved: int = 0     # device bytes charged to the budget in preparation
 
     def release_result(self) -> None:
         """Hand the result's pinned host buffer back to the server's pool
@@ -136,22 +145,86 @@ class ContractionServer:
         self._lock = threading.Lock()
         self._inbox = collections.deque()
         self.ticks_launched = 0
+        # A backend with `prepare` (staging and planning per request) gets a
+        # preparation thread: requests are prepared as they arrive, off the
+        # loop that completes, admits and launches ticks.
+        self._prepare = getattr(backend, "prepare", None)
+        self._prep_q = collections.deque()
+        self._prep_cv = threading.Condition()
+        self._budget_cv = threading.Condition()  # guards `used` while preparation runs
+        self._prep_stop = False
+        self._prep_thread = None
+        if self._prepare is not None:
+            self._prep_thread = threading.Thread(target=self._prep_loop, name="qs-serve-prepare", daemon=True)
+            self._prep_thread.start()
+
+    def _prep_loop(self) -> None:
+        while True:
+            with self._prep_cv:
+                while not self._prep_q and not self._prep_stop:
+                    self._prep_cv.wait()
+                if self._prep_stop:
+                    return
+                r = self._prep_q.popleft()
+            try:
+                if self._reserve(r):
+                    self._prepare(r)
+            except Exception as e:  # the request fails alone; the loop reports it
+                r.error = f"preparation failed: {e}"
+            r.prepared = True
+
+    def _reserve(self, r: ContractRequest) -> bool:
+        """Charge a request's device bytes to the budget before it is staged
+        (waiting for completions while it does not fit); False for a request
+        larger than the budget, which fails."""
+        b = self.request_bytes(r)
+        with self._budget_cv:
+            if b > self.budget - sum(self.residents.values()):
+                r.error = f"request needs {b} bytes, more than the budget"
+                return False
+            while self.used + b + self.be.cached_bytes() > self.budget:
+                self.be.evict(self.used + b + self.be.cached_bytes() - self.budget)
+                if self.used + b + self.be.cached_bytes() <= self.budget or self._prep_stop:
+                    break
+                self._budget_cv.wait(0.01)
+            self.used += b
+            self.peak_used = max(self.peak_used, self.used)
+        r._reserved = b
+        return True
+
+    def close(self) -> None:
+        """Stop the preparation thread (requests not yet prepared are
+        prepared by the loop when admitted)."""
+        if self._prep_thread is not None:
+            with self._prep_cv:
+                self._prep_stop = True
+                self._prep_cv.notify()
+            self._prep_thread.join()
+            self._prep_thread = None
+            self._prepare = None
 
     # ------------------------------------------------------------ API ---
     def put_resident(self, key, array) -> None:
         nbytes = self.be.put_resident(key, array)
-        self.residents[key] = nbytes
-        self.used += nbytes
-        self.peak_used = max(self.peak_used, self.used)
+        with self._budget_cv:
+            self.residents[key] = nbytes
+            self.used += nbytes
+            self.peak_used = max(self.peak_used, self.used)
 
     def drop_resident(self, key) -> None:
         self.be.drop_resident(key)
-        self.used -= self.residents.pop(key)
+        with self._budget_cv:
+            self.used -= self.residents.pop(key)
+            self._budget_cv.notify_all()
 
     def submit(self, req: ContractRequest, now: Optional[float] = None) -> ContractRequest:
         req.arrival = time.perf_counter() if now is None else now
         with self._lock:
             self._inbox.append(req)
+        if self._prepare is not None:
+            with self._prep_cv:
+                self._prep_q.append(req)
+                self._prep_cv.notify()
         return req
 
     def request_bytes(self, req: ContractRequest) -> int:
@@ -175,16 +248,40 @@ class ContractionServer:
                     self.completed.append(r)
                     if self.on_done is not None:
                         self.on_done(r)
-                self.used -= t.bytes
+                with self._budget_cv:
+                    self.used -= t.bytes
+                    self._budget_cv.notify_all()
                 busy = True
             else:
                 still.append(t)
         self.inflight = still
         # 2. admission (FIFO; a request that does not fit waits, later ones too)
         if self.pending and len(self.inflight) < self.max_ticks:
-            batch, nbytes, work = [], 0, 0.0
+            batch, nbytes, work, reserved = [], 0, 0.0, 0  # reserved: bytes charged in preparation
             while self.pending and len(batch) < self.max_tick_requests:
                 r = self.pending[0]
+                if self._prepare is not None:
+                    if not r.prepared:
+                        break  # FIFO: wait for its preparation
+                    if r.error is not None:  # rejected or failed in preparation
+                        self.pending.popleft()
+                        with self._budget_cv:
+                            self.used -= r._reserved
+                            self._budget_cv.notify_all()
+                        r._reserved = 0
+                        r.done = time.perf_counter()
+                        self.completed.append(r)
+                        continue
+                    f = r.flops(self.be.shape_of) if self.max_tick_flops else 0.0
+                    if self.max_tick_flops and batch and work + f > self.max_tick_flops:
+                        break
+                    if self.max_tick_bytes and batch and nbytes + r._reserved > self.max_tick_bytes:
+                        break
+                    batch.append(self.pending.popleft())
+                    reserved += r._reserved
+                    nbytes += r._reserved
+                    work += f
+                    continue
                 b = self.request_bytes(r)
                 f = r.flops(self.be.shape_of) if self.max_tick_flops else 0.0
                 if self.max_tick_flops and batch and work + f > self.max_tick_flops:
@@ -209,8 +306,9 @@ class ContractionServer:
                 now = time.perf_counter()
                 for r in batch:
                     r.admitted = now
-                self.used += nbytes
-                self.peak_used = max(self.peak_used, self.used)
+                with self._budget_cv:
+                    self.used += nbytes - reserved
+                    self.peak_used = max(self.peak_used, self.used)
                 handle = self.be.launch_tick(batch)
                 self.inflight.append(Tick(batch, nbytes, handle, now))
                 self.ticks_launched += 1
@@ -354,6 +452,12 @@ class DeviceBackend:
         self.plan_cache = collections.OrderedDict()  # signature -> [plans], LRU first
         self._cached_bytes = 0
         self.grouped = grouped
+        # The server's preparation thread and its loop share the arenas and
+        # the plan cache (_lock) and call into the library (_qs_lock: one
+        # library call at a time; a plan or a grouped launch takes tens of
+        # microseconds).
+        self._lock = threading.RLock()
+        self._qs_lock = threading.RLock()
         # host seconds per launch phase, and device milliseconds per tick
         self.timing = collections.Counter()
         self.tick_gpu_ms = []
@@ -378,11 +482,11 @@ class DeviceBackend:
     def _device(self, n, tdt):
         return self._take(self.dev_arena, self.dev_mem, n, tdt, "device")
 
-    @staticmethod
-    def _give(handle):
+    def _give(self, handle):
         arena, off = handle
         if arena is not None:
-            arena.free(off)
+            with self._lock:
+                arena.free(off)
 
     def _unpin(self, handle):
         self._give(handle)
@@ -427,86 +531,107 @@ class DeviceBackend:
     def _signature(self, r, sa, sb, sc):
         return (np.dtype(r.dtype).str, sa, tuple(r.indA), sb, tuple(r.indB), sc, tuple(r.indC))
 
+    def prepare(self, r: ContractRequest) -> None:
+        """Stage one request for its tick: device blocks for A, B and C,
+        pinned copies of host operands, and its plan (from the plan cache
+        or `plan_contract`).  The server runs this on its preparation
+        thread as requests arrive, so the loop that admits and launches
+        ticks does none of it; `launch_tick` only enqueues device work."""
+        torch = self.torch
+        clk = time.perf_counter
+        t0 = clk()
+        tdt = self._tdtype[np.dtype(r.dtype)]
+        staged, dev_blocks, copies_in = [], [], []
+
+        def device_copy_of(x):
+            h = torch.from_numpy(np.asfortranarray(x).ravel(order="F"))
+            if not h.is_pinned():
+                with self._lock:
+                    buf, h2 = self._pinned(h.numel(), tdt)
+                h2.copy_(h)
+                staged.append(buf)
+                h = h2
+            with self._lock:
+                dh, t = self._device(h.numel(), tdt)
+            dev_blocks.append(dh)
+            copies_in.append((t, h))
+            return t
+
+        ops = []
+        for x in (r.A, r.B):
+            if isinstance(x, str):
+                t, shp, _ = self.resident[x]
+                ops.append((t, shp))
+            else:
+                ops.append((device_copy_of(x), x.shape))
+        sc = r.c_shape(self.shape_of)
+        ncs = int(np.prod(sc)) if sc else 1
+        zero_c = r.C0 is None
+        if zero_c:
+            with self._lock:
+                dh, Cd = self._device(ncs, tdt)
+            dev_blocks.append(dh)
+        else:
+            Cd = device_copy_of(r.C0)
+        t1 = clk()
+        Av, Bv, Cv = self._view(ops[0][0], ops[0][1]), self._view(ops[1][0], ops[1][1]), self._view(Cd, sc)
+        key = self._signature(r, tuple(ops[0][1]), tuple(ops[1][1]), tuple(sc))
+        plan = None
+        with self._lock:
+            if self.plan_cache.get(key):
+                plan = self.plan_cache[key].pop()
+                self._cached_bytes -= plan.workspace_bytes
+        with self._qs_lock:
+            if plan is not None:
+                plan.rebind(Av, Bv, Cv)
+            else:
+                plan = self.qs.plan_contract(Cv, Av, r.indA, Bv, r.indB, r.indC)
+        with self._lock:
+            out_buf, host_out = self._pinned(ncs, tdt)
+            self.timing["stage"] += t1 - t0
+            self.timing["plan"] += clk() - t1
+        r._prep = {"item": (r, key, plan, Cd, host_out, ops, sc, out_buf, staged, dev_blocks),
+                   "copies_in": copies_in, "alpha": r.alpha, "beta": r.beta if not zero_c else 0.0}
+
     def launch_tick(self, batch, grouped: Optional[bool] = None):
-        """Prepare the whole tick on the host (device buffers from the
-        stream's caching allocator, pinned staging, plans), then enqueue its
-        device work as one burst on the tick's stream: uploads, one grouped
-        execute (or one execute per plan), downloads, an event."""
+        """Enqueue a tick's device work as one burst on the tick's stream:
+        uploads, one grouped execute (or one execute per plan), downloads,
+        an event.  Requests not yet prepared are prepared here."""
         torch = self.torch
         grouped = self.grouped if grouped is None else grouped
         st = self.streams[self.next_stream % len(self.streams)]
         self.next_stream += 1
         T = self.timing
         clk = time.perf_counter
-        items, copies_in, plans, alphas, betas = [], [], [], [], []
-        t0 = clk()
+        for r in batch:
+            if getattr(r, "_prep", None) is None:
+                self.prepare(r)
+        items = [r._prep["item"] for r in batch]
+        plans = [it[2] for it in items]
+        alphas = [r._prep["alpha"] for r in batch]
+        betas = [r._prep["beta"] for r in batch]
         with torch.cuda.stream(st):
-            for r in batch:
-                tdt = self._tdtype[np.dtype(r.dtype)]
-                staged, dev_blocks = [], []
-
-                def device_copy_of(x):
-                    h = torch.from_numpy(np.asfortranarray(x).ravel(order="F"))
-                    if not h.is_pinned():
-                        buf, h2 = self._pinned(h.numel(), tdt)
-                        h2.copy_(h)
-                        staged.append(buf)
-                        h = h2
-                    dh, t = self._device(h.numel(), tdt)
-                    dev_blocks.append(dh)
-                    copies_in.append((t, h))
-                    return t
-
-                ops = []
-                for x in (r.A, r.B):
-                    if isinstance(x, str):
-                        t, shp, _ = self.resident[x]
-                        ops.append((t, shp))
-                    else:
-                        ops.append((device_copy_of(x), x.shape))
-                sc = r.c_shape(self.shape_of)
-                ncs = int(np.prod(sc)) if sc else 1
-                zero_c = r.C0 is None
-                if zero_c:
-                    dh, Cd = self._device(ncs, tdt)
-                    dev_blocks.append(dh)
-                else:
-                    Cd = device_copy_of(r.C0)
-                t1 = clk()
-                T["stage"] += t1 - t0
-                Av, Bv, Cv = self._view(ops[0][0], ops[0][1]), self._view(ops[1][0], ops[1][1]), self._view(Cd, sc)
-                key = self._signature(r, tuple(ops[0][1]), tuple(ops[1][1]), tuple(sc))
-                if self.plan_cache.get(key):
-                    plan = self.plan_cache[key].pop()
-                    self._cached_bytes -= plan.workspace_bytes
-                    plan.rebind(Av, Bv, Cv)
-                else:
-                    plan = self.qs.plan_contract(Cv, Av, r.indA, Bv, r.indB, r.indC)
-                t0 = clk()
-                T["plan"] += t0 - t1
-                out_buf, host_out = self._pinned(ncs, tdt)
-                plans.append(plan)
-                alphas.append(r.alpha)
-                betas.append(r.beta if not zero_c else 0.0)
-                items.append((r, key, plan, Cd, host_out, ops, sc, out_buf, staged, dev_blocks))
-            # device work, one burst
             ev0 = torch.cuda.Event(enable_timing=True)
             ev0.record(st)
-            for t, h in copies_in:
-                t.copy_(h, non_blocking=True)
+            for r in batch:
+                for t, h in r._prep["copies_in"]:
+                    t.copy_(h, non_blocking=True)
             t3 = clk()
-            if grouped:
-                g = self.qs.ContractGroup(plans, mode="persistent")
-                g.execute(alphas, betas, stream=st)
-            else:
-                g = None
-                for p, a, b in zip(plans, alphas, betas):
-                    self.qs.execute(p, a, b, stream=st)
+            with self._qs_lock:
+                if grouped:
+                    g = self.qs.ContractGroup(plans, mode="persistent")
+                    g.execute(alphas, betas, stream=st)
+                else:
+                    g = None
+                    for p, a, b in zip(plans, alphas, betas):
+                        self.qs.execute(p, a, b, stream=st)
             T["execute"] += clk() - t3
             for it in items:
                 it[4].copy_(it[3], non_blocking=True)
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(st)
+        for r in batch:
+            r._prep = None
         T["ticks"] += 1
         return {"event": ev, "start": ev0, "items": items, "group": g, "stream": st}
 
@@ -517,7 +642,8 @@ class DeviceBackend:
         h["event"].synchronize()
         self.tick_gpu_ms.append(h["start"].elapsed_time(h["event"]))
         if h["group"] is not None:
-            h["group"].release()
+            with self._qs_lock:
+                h["group"].release()
         # Each result is a view of a pooled pinned buffer, handed to the
         # request; ContractRequest.release_result() returns the buffer.
         for (r, key, plan, Cd, host_out, ops, sc, out_buf, staged, dev_blocks) in h["items"]:
@@ -528,19 +654,22 @@ class DeviceBackend:
                 self._unpin(b)
             for b in dev_blocks:  # the tick's event has fired: the device is done with them
                 self._give(b)
-            plan.detach_storage()
-            self.plan_cache.setdefault(key, []).append(plan)
-            self.plan_cache.move_to_end(key)
-            self._cached_bytes += plan.workspace_bytes
+            with self._qs_lock:
+                plan.detach_storage()
+            with self._lock:
+                self.plan_cache.setdefault(key, []).append(plan)
+                self.plan_cache.move_to_end(key)
+                self._cached_bytes += plan.workspace_bytes
         h["items"] = []
 
     def clear_plan_cache(self) -> None:
         """Release every cached plan."""
-        for plans in self.plan_cache.values():
-            for p in plans:
-                p.release()
-        self.plan_cache.clear()
-        self._cached_bytes = 0
+        with self._lock, self._qs_lock:
+            for plans in self.plan_cache.values():
+                for p in plans:
+                    p.release()
+            self.plan_cache.clear()
+            self._cached_bytes = 0
 
     def cached_bytes(self) -> int:
         """Device workspace held by idle cached plans."""
@@ -549,12 +678,13 @@ class DeviceBackend:
     def evict(self, nbytes: int) -> None:
         """Release least recently used cached plans until nbytes are freed."""
         freed = 0
-        while freed < nbytes and self.plan_cache:
-            key, plans = next(iter(self.plan_cache.items()))
-            while plans and freed < nbytes:
-                p = plans.pop()
-                freed += p.workspace_bytes
-                self._cached_bytes -= p.workspace_bytes
-                p.release()
-            if not plans:
-                del self.plan_cache[key]
+        with self._lock, self._qs_lock:
+            while freed < nbytes and self.plan_cache:
+                key, plans = next(iter(self.plan_cache.items()))
+                while plans and freed < nbytes:
+                    p = plans.pop()
+                    freed += p.workspace_bytes
+                    self._cached_bytes -= p.workspace_bytes
+                    p.release()
+                if not plans:
+                    del self.plan_cache[key]
