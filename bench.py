@@ -551,6 +551,7 @@ def run_serving(args):
                          "arena_fallbacks": dict(be.fallbacks)}
             for key in residents:
                 srv.drop_resident(key)
+            srv.close()
             del srv
             torch.cuda.synchronize()
         result["rates"].append(row)
