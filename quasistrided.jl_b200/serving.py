@@ -72,6 +72,7 @@ class ContractRequest:
     _prep: Any = None      # the backend's staged buffers and plan, once prepared
     prepared: bool = False
     _reserved: int = 0     # device bytes charged to the budget in preparation
+    _pstate: int = 0       # preparation: 0 queued, 1 taken (by the thread or the loop)
 
     def release_result(self) -> None:
         """Hand the result's pinned host buffer back to the server's pool
@@ -166,17 +167,32 @@ class ContractionServer:
                 if self._prep_stop:
                     return
                 r = self._prep_q.popleft()
-            try:
-                if self._reserve(r):
-                    self._prepare(r)
-            except Exception as e:  # the request fails alone; the loop reports it
-                r.error = f"preparation failed: {e}"
-            r.prepared = True
+                if r._pstate != 0:  # the loop took it
+                    continue
+                r._pstate = 1
+            self._prepare_now(r, wait=True)
 
-    def _reserve(self, r: ContractRequest) -> bool:
+    def _prepare_now(self, r: ContractRequest, wait: bool) -> bool:
+        """Reserve and prepare r; False (r untouched, back in the queue's
+        state) when wait is False and its bytes do not fit yet."""
+        try:
+            ok = self._reserve(r, wait)
+            if ok is None:
+                with self._prep_cv:
+                    r._pstate = 0
+                return False
+            if ok:
+                self._prepare(r)
+        except Exception as e:  # the request fails alone; the loop reports it
+            r.error = f"preparation failed: {e}"
+        r.prepared = True
+        return True
+
+    def _reserve(self, r: ContractRequest, wait: bool = True):
         """Charge a request's device bytes to the budget before it is staged
-        (waiting for completions while it does not fit); False for a request
-        larger than the budget, which fails."""
+        (waiting for completions while it does not fit, or returning None at
+        once when wait is False); False for a request larger than the
+        budget, which fails."""
         b = self.request_bytes(r)
         with self._budget_cv:
             if b > self.budget - sum(self.residents.values()):
@@ -186,6 +202,8 @@ class ContractionServer:
                 self.be.evict(self.used + b + self.be.cached_bytes() - self.budget)
                 if self.used + b + self.be.cached_bytes() <= self.budget or self._prep_stop:
                     break
+                if not wait:
+                    return None
                 self._budget_cv.wait(0.01)
             self.used += b
             self.peak_used = max(self.peak_used, self.used)
@@ -262,7 +280,14 @@ class ContractionServer:
                 r = self.pending[0]
                 if self._prepare is not None:
                     if not r.prepared:
-                        break  # FIFO: wait for its preparation
+                        # FIFO: wait for its preparation, or do it here when
+                        # the preparation thread has not started it
+                        with self._prep_cv:
+                            mine = r._pstate == 0
+                            if mine:
+                                r._pstate = 1
+                        if not (mine and self._prepare_now(r, wait=False)):
+                            break
                     if r.error is not None:  # rejected or failed in preparation
                         self.pending.popleft()
                         with self._budget_cv:

@@ -5,6 +5,10 @@ device is replaced by a fake backend whose ticks complete after a few polls
 and compute with numpy."""
 import importlib
 
+import collections
+import threading
+import time
+
 import numpy as np
 import pytest
 
@@ -195,3 +199,46 @@ def test_tick_work_cap(sv):
     srv.drain(timeout=30)
     assert all(len(t) <= 2 for t in be.launched)  # two 1024-flop requests per tick
     assert sum(len(t) for t in be.launched) == 12
+
+
+class PreparingBackend(FakeBackend):
+    """A backend with `prepare`: the server stages requests on its
+    preparation thread (or in the loop when the thread has not started one)
+    before admitting them; a slow prepare makes both paths run."""
+
+    def __init__(self, polls=2, delay=2e-4):
+        super().__init__(polls)
+        self.delay = delay
+        self.prepared = collections.Counter()
+        self.threads = set()
+        self.lock = threading.Lock()
+
+    def prepare(self, r):
+        time.sleep(self.delay)
+        with self.lock:
+            self.prepared[id(r)] += 1
+            self.threads.add(threading.current_thread().name)
+        r._prep = True
+
+    def launch_tick(self, batch, grouped=True):
+        assert all(r._prep for r in batch)  # admitted only once prepared
+        return super().launch_tick(batch, grouped)
+
+
+def test_preparation_thread_budget_fifo_and_results(sv):
+    rng = np.random.default_rng(4)
+    be = PreparingBackend()
+    per = 3 * 8 * 8 * 8
+    srv = sv.ContractionServer(be, hbm_budget_bytes=5 * per, max_ticks=3, max_tick_requests=2)
+    reqs = mk(sv, rng, 60)
+    offsets = np.cumsum(rng.exponential(3e-4, 60))
+    srv.replay(reqs, offsets, timeout=60)
+    srv.close()
+    assert all(be.prepared[id(r)] == 1 for r in reqs)   # each prepared exactly once
+    assert srv.peak_used <= 5 * per                      # preparation is charged to the budget
+    order = [i for tick in be.launched for i in tick]
+    assert order == [id(r) for r in reqs]                # admitted in arrival order
+    for r in reqs:
+        assert r.error is None
+        assert np.allclose(r.result, einsum_labels(r.A, r.indA, r.B, r.indB, r.indC) * r.alpha)
+    assert srv.used == 0
