@@ -643,7 +643,7 @@ class DeviceBackend:
                     t.copy_(h, non_blocking=True)
             t3 = clk()
             with self._qs_lock:
-                if grouped:
+                if grouped and len(plans) > 1:  # one plan: its own execute, no group tables
                     g = self.qs.ContractGroup(plans, mode="persistent")
                     g.execute(alphas, betas, stream=st)
                 else:
