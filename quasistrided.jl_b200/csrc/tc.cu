@@ -1892,22 +1892,35 @@ __global__ void __launch_bounds__(256) oz_prep_grouped(const ZeroJob *jobs, int 
 // blocks from b0; pass 1 skips the K blocks past K.  A group packs chunk by
 // chunk (pass 1, pass 2, next chunk), each chunk's operands small enough
 // that pass 2 re-reads them from L2.
+// The block's job in shared memory (one coalesced load of the whole record,
+// so the pass reads its arguments from shared memory instead of a chain of
+// dependent loads from the job table), and the block's (r0, k0).
+__device__ __forceinline__ void stage_pack_job(const PackJob *jobs, const int *jobmap, int b, PackJob &sj,
+                                               int64_t &r0, int64_t &k0) {
+  static_assert(sizeof(PackJob) % 8 == 0, "PackJob copies as 8-byte words");
+  const uint64_t *src = reinterpret_cast<const uint64_t *>(jobs + __ldg(jobmap + b));
+  if (threadIdx.x < sizeof(PackJob) / 8) reinterpret_cast<uint64_t *>(&sj)[threadIdx.x] = __ldg(src + threadIdx.x);
+  __syncthreads();
+  const int lb = b - sj.block_start;
+  r0 = (int64_t)(lb % sj.gx) * kPackRows;
+  k0 = (int64_t)(lb / sj.gx) * kPackK;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs, const int *jobmap, int b0) {
-  const int b = b0 + (int)blockIdx.x;
-  const PackJob &j = jobs[__ldg(jobmap + b)];
-  const int lb = b - j.block_start;
-  const int64_t r0 = (int64_t)(lb % j.gx) * kPackRows, k0 = (int64_t)(lb / j.gx) * kPackK;
-  if (k0 >= j.pa.K) return;
-  oz_rowmax_block<KIND>(j.pa, r0, k0);
+  __shared__ PackJob sj;
+  int64_t r0, k0;
+  stage_pack_job(jobs, jobmap, b0 + (int)blockIdx.x, sj, r0, k0);
+  if (k0 >= sj.pa.K) return;
+  oz_rowmax_block<KIND>(sj.pa, r0, k0);
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, const int *jobmap, int b0) {
-  const int b = b0 + (int)blockIdx.x;
-  const PackJob &j = jobs[__ldg(jobmap + b)];
-  const int lb = b - j.block_start;
-  oz_digit_block<KIND>(j.pa, (int64_t)(lb % j.gx) * kPackRows, (int64_t)(lb / j.gx) * kPackK);
+  __shared__ PackJob sj;
+  int64_t r0, k0;
+  stage_pack_job(jobs, jobmap, b0 + (int)blockIdx.x, sj, r0, k0);
+  oz_digit_block<KIND>(sj.pa, r0, k0);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, const int *jobmap) {
