@@ -122,39 +122,47 @@ __device__ __forceinline__ int tcol(int k) {
   return (k & ~(W - 1)) | ((k + k / W) & (W - 1));
 }
 
-// Real operands stored as S: each thread keeps the offset of its fixed row
-// (or K index) in a register and issues all of its loads independently.
+// Real operands stored as S.  The block's 32 row offsets and KT K offsets
+// are staged in shared memory first (two coalesced loads), so each element's
+// load waits on a shared-memory read rather than on an offset load from
+// L1/L2; every thread then issues its loads independently, coalesced along
+// whichever of rows / K is X's unit-stride axis.  Every thread of the block
+// calls it.
 template <class T, class S, int KT>
 __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, int64_t k0,
                                                T (*tile)[KT + 1]) {
+  __shared__ int64_t s_ro[32], s_ko[KT];
   const int tid = threadIdx.x;
   constexpr int PER = 32 * KT / 256;
-  const S *X = static_cast<const S *>(a.X) + a.Xbase;
+  for (int i = tid; i < KT; i += 256) {
+    const int64_t k = k0 + i;
+    s_ko[i] = k < a.K ? __ldg(a.offK + k) : INT64_MIN;
+  }
+  if (tid < 32) {
+    const int64_t r = pack_row(a, r0 + tid);
+    s_ro[tid] = r < a.rows ? a.Xbase + __ldg(a.offR + r) : INT64_MIN;
+  }
+  __syncthreads();
+  const S *X = static_cast<const S *>(a.X);
   if (a.rfast) {
     const int rr = tid & 31, kb = tid >> 5;
-    const int64_t r = pack_row(a, r0 + rr);
-    const bool rok = r < a.rows;
-    const int64_t ro = rok ? __ldg(a.offR + r) : 0;
+    const int64_t ro = s_ro[rr];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int kk = kb + 8 * i;
-      const int64_t k = k0 + kk;
-      const bool ok = rok && k < a.K;
-      const int64_t ko = ok ? __ldg(a.offK + k) : 0;
+      const int64_t ko = s_ko[kk];
+      const bool ok = ro != INT64_MIN && ko != INT64_MIN;
       tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
     }
   } else {
     constexpr int RSTEP = 256 / KT;
     const int kk = tid % KT, rb = tid / KT;
-    const int64_t k = k0 + kk;
-    const bool kok = k < a.K;
-    const int64_t ko = kok ? __ldg(a.offK + k) : 0;
+    const int64_t ko = s_ko[kk];
 #pragma unroll
     for (int i = 0; i < PER; ++i) {
       const int rr = rb + RSTEP * i;
-      const int64_t r = pack_row(a, r0 + rr);
-      const bool ok = kok && r < a.rows;
-      const int64_t ro = ok ? __ldg(a.offR + r) : 0;
+      const int64_t ro = s_ro[rr];
+      const bool ok = ko != INT64_MIN && ro != INT64_MIN;
       tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
     }
   }
