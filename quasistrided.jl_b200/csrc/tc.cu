@@ -122,15 +122,56 @@ __device__ __forceinline__ int tcol(int k) {
   return (k & ~(W - 1)) | ((k + k / W) & (W - 1));
 }
 
-// Real operands stored as S.  The block's 32 row offsets and KT K offsets
-// are staged in shared memory first (two coalesced loads), so each element's
-// load waits on a shared-memory read rather than on an offset load from
-// L1/L2; every thread then issues its loads independently, coalesced along
-// whichever of rows / K is X's unit-stride axis.  Every thread of the block
-// calls it.
+// Real operands stored as S: each thread keeps the offset of its fixed row
+// (or K index) in a register and issues all of its loads independently.
 template <class T, class S, int KT>
 __device__ __forceinline__ void load_tile_real(const PackArgs &a, int64_t r0, int64_t k0,
                                                T (*tile)[KT + 1]) {
+  const int tid = threadIdx.x;
+  constexpr int PER = 32 * KT / 256;
+  const S *X = static_cast<const S *>(a.X) + a.Xbase;
+  if (a.rfast) {
+    const int rr = tid & 31, kb = tid >> 5;
+    const int64_t r = pack_row(a, r0 + rr);
+    const bool rok = r < a.rows;
+    const int64_t ro = rok ? __ldg(a.offR + r) : 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int kk = kb + 8 * i;
+      const int64_t k = k0 + kk;
+      const bool ok = rok && k < a.K;
+      const int64_t ko = ok ? __ldg(a.offK + k) : 0;
+      tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+    }
+  } else {
+    constexpr int RSTEP = 256 / KT;
+    const int kk = tid % KT, rb = tid / KT;
+    const int64_t k = k0 + kk;
+    const bool kok = k < a.K;
+    const int64_t ko = kok ? __ldg(a.offK + k) : 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+      const int rr = rb + RSTEP * i;
+      const int64_t r = pack_row(a, r0 + rr);
+      const bool ok = kok && r < a.rows;
+      const int64_t ro = ok ? __ldg(a.offR + r) : 0;
+      tile[rr][tcol<KT>(kk)] = ok ? (T)__ldg(X + ro + ko) : (T)0;
+    }
+  }
+}
+
+// The same with the block's 32 row offsets and KT K offsets staged in
+// shared memory first (two coalesced loads), so each element's
+// load waits on a shared-memory read rather than on an offset load from
+// L1/L2; every thread then issues its loads independently, coalesced along
+// whichever of rows / K is X's unit-stride axis.  Every thread of the block
+// calls it.  It pays in grouped launches (short blocks of many problems:
+// 6 % on the 2000-block step) and loses on one large operand (the offsets
+// are L1 broadcasts there and the barrier delays each block's loads: the
+// pack of the permuted 4-index contraction took 0.18 ms instead of 0.12).
+template <class T, class S, int KT>
+__device__ __forceinline__ void load_tile_real_staged(const PackArgs &a, int64_t r0, int64_t k0,
+                                                      T (*tile)[KT + 1]) {
   __shared__ int64_t s_ro[32], s_ko[KT];
   const int tid = threadIdx.x;
   constexpr int PER = 32 * KT / 256;
@@ -270,21 +311,29 @@ __host__ __device__ inline int pack_kind_of(const PackArgs &a) {
   return kPackAny;
 }
 
-template <int KIND>
+// STAGE: the real loaders with their offsets staged in shared memory
+// (grouped launches).
+template <int KIND, bool STAGE>
 __device__ __forceinline__ void pack_load(const PackArgs &a, int64_t r0, int64_t k0,
                                           double (*tile)[kPackK + 1]) {
-  if constexpr (KIND == kPackF64) load_tile_real<double, double, kPackK>(a, r0, k0, tile);
-  else if constexpr (KIND == kPackF32) load_tile_real<double, float, kPackK>(a, r0, k0, tile);
-  else load_tile<double, kPackK>(a, r0, k0, tile);
+  if constexpr (KIND == kPackF64) {
+    if constexpr (STAGE) load_tile_real_staged<double, double, kPackK>(a, r0, k0, tile);
+    else load_tile_real<double, double, kPackK>(a, r0, k0, tile);
+  } else if constexpr (KIND == kPackF32) {
+    if constexpr (STAGE) load_tile_real_staged<double, float, kPackK>(a, r0, k0, tile);
+    else load_tile_real<double, float, kPackK>(a, r0, k0, tile);
+  } else {
+    load_tile<double, kPackK>(a, r0, k0, tile);
+  }
 }
 
 // Pass 1: each row's max magnitude as the bit pattern of |x| (for
 // non-negative doubles the integer order is the value order, and a NaN or
 // Inf sorts above every finite value).  8 threads per row.
-template <int KIND>
+template <int KIND, bool STAGE>
 __device__ __forceinline__ void oz_rowmax_block(const PackArgs &a, int64_t r0, int64_t k0) {
   __shared__ double tile[kPackRows][kPackK + 1];
-  pack_load<KIND>(a, r0, k0, tile);
+  pack_load<KIND, STAGE>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, part = threadIdx.x & 7;
   unsigned long long m = 0;
@@ -329,10 +378,10 @@ __device__ __forceinline__ RowScale row_scale(unsigned long long mb, int s) {
 // Pass 2: the digit planes of one 32-row x 128-K block (the balanced
 // base-256 digits described above).  Thread (row, c) writes the 16 digits
 // of K values c*16 .. c*16 + 15 of its row into each plane.
-template <int KIND>
+template <int KIND, bool STAGE>
 __device__ __forceinline__ void oz_digit_block(const PackArgs &a, int64_t r0, int64_t k0) {
   __shared__ double tile[kPackRows][kPackK + 1];
-  pack_load<KIND>(a, r0, k0, tile);
+  pack_load<KIND, STAGE>(a, r0, k0, tile);
   __syncthreads();
   const int row = threadIdx.x >> 3, c = threadIdx.x & 7;
   const int64_t grow = pack_row(a, r0 + row);
@@ -402,14 +451,14 @@ template <int KIND>
 __global__ void __launch_bounds__(256, 6) oz_rowmax_kernel(const __grid_constant__ PackArgs a, int nrb) {
   int64_t r0, k0;
   pack_block_coords(blockIdx.x, nrb, r0, k0);
-  oz_rowmax_block<KIND>(a, r0, k0);
+  oz_rowmax_block<KIND, false>(a, r0, k0);
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(256, 4) oz_digit_kernel(const __grid_constant__ PackArgs a, int nrb) {
   int64_t r0, k0;
   pack_block_coords(blockIdx.x, nrb, r0, k0);
-  oz_digit_block<KIND>(a, r0, k0);
+  oz_digit_block<KIND, false>(a, r0, k0);
 }
 
 // Pass 1 and pass 2 of one operand: blocks cover rows_pad x kblocks * 128
@@ -1920,7 +1969,7 @@ __global__ void __launch_bounds__(256, 6) oz_rowmax_grouped(const PackJob *jobs,
   int64_t r0, k0;
   stage_pack_job(jobs, jobmap, b0 + (int)blockIdx.x, sj, r0, k0);
   if (k0 >= sj.pa.K) return;
-  oz_rowmax_block<KIND>(sj.pa, r0, k0);
+  oz_rowmax_block<KIND, true>(sj.pa, r0, k0);
 }
 
 template <int KIND>
@@ -1928,7 +1977,7 @@ __global__ void __launch_bounds__(256, 4) oz_digit_grouped(const PackJob *jobs, 
   __shared__ PackJob sj;
   int64_t r0, k0;
   stage_pack_job(jobs, jobmap, b0 + (int)blockIdx.x, sj, r0, k0);
-  oz_digit_block<KIND>(sj.pa, r0, k0);
+  oz_digit_block<KIND, true>(sj.pa, r0, k0);
 }
 
 __global__ void __launch_bounds__(256) bf16_pack_grouped(const PackJob *jobs, const int *jobmap) {
