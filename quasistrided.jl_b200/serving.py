@@ -562,6 +562,12 @@ class DeviceBackend:
         or `plan_contract`).  The server runs this on its preparation
         thread as requests arrive, so the loop that admits and launches
         ticks does none of it; `launch_tick` only enqueues device work."""
+        # The preparation thread's current device is not the loop's: plans
+        # and their workspace go to this backend's device.
+        with self.torch.cuda.device(self.dev):
+            self._prepare_on_device(r)
+
+    def _prepare_on_device(self, r: ContractRequest) -> None:
         torch = self.torch
         clk = time.perf_counter
         t0 = clk()
